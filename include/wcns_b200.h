@@ -1,0 +1,102 @@
+/*
+ * wcns_b200.h -- C ABI of the B200 (sm_100a) implementation of WCNS's
+ * per-step residual (RHS) and implicit LU-SGS update (LHS) on multi-block
+ * structured grids.
+ *
+ * The reference exposes this path as argument-less Fortran subroutines that
+ * act on module globals and are called from its time loop (Main.f90:79-127).
+ * Each entry point below replaces one of those calls; a Fortran driver binds
+ * them with iso_c_binding.  All functions return 0 on
+ * success and a nonzero WcnsStatus otherwise; wcns_last_error() gives the
+ * message.  No exception crosses this boundary.  One host thread drives one
+ * context; all device work of a context is ordered on the context's stream.
+ *
+ * Array conventions (host side): per block and per variable one double array
+ * in the reference's ghosted index space (-2:n+3 in every direction), i
+ * fastest, i.e. (ni+6)*(nj+6)*(nk+6) values; coordinates are interior only,
+ * ni*nj*nk values, i fastest.  Block numbers are 1-based as in the reference.
+ */
+#ifndef WCNS_B200_H
+#define WCNS_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The param.dat namelist values the path reads ($inflow, $step, $flowtype,
+ * $technic; read_parameter, PreProcess.f90:80-159). */
+typedef struct WcnsParams {
+    double moo, attack, sideslip, reynolds, tref, twall;
+    double cfl, timedt_rate, efix, csrv;
+    int nvis, nscheme, nflux, flags;
+} WcnsParams;
+
+typedef struct WcnsContext WcnsContext;
+
+typedef enum WcnsStatus {
+    WCNS_OK = 0,
+    WCNS_ERR_ARGUMENT = 1,   /* invalid input (replaces the reference's stop) */
+    WCNS_ERR_ROE = 2,        /* Roe flux c^2 <= 0 (flux.f90:179-182) */
+    WCNS_ERR_UPDATE = 3,     /* too many non-physical points (Sub2.f90:781-785) */
+    WCNS_ERR_CUDA = 4,
+    WCNS_ERR_UNSUPPORTED = 5 /* BC type or field not handled (BC.f90:203-205) */
+} WcnsStatus;
+
+/* Field identifiers for wcns_get_field / wcns_set_field. */
+enum {
+    WCNS_F_R = 0, WCNS_F_U, WCNS_F_V, WCNS_F_W, WCNS_F_P, WCNS_F_T,
+    WCNS_F_DQ1, WCNS_F_DQ2, WCNS_F_DQ3, WCNS_F_DQ4, WCNS_F_DQ5,
+    WCNS_F_DTDT, WCNS_F_SRA, WCNS_F_SRB, WCNS_F_SRC, WCNS_F_SRVA, WCNS_F_SRVB, WCNS_F_SRVC,
+    WCNS_F_KCX, WCNS_F_KCY, WCNS_F_KCZ, WCNS_F_ETX, WCNS_F_ETY, WCNS_F_ETZ,
+    WCNS_F_CTX, WCNS_F_CTY, WCNS_F_CTZ, WCNS_F_VOL
+};
+
+/* Pre-processing.  Replaces read_bc_parallel + analyze_bc + set_bc_index
+ * (parallel.f90:852-1300, PreProcess.f90:2543-2572), build_nppos_list_ex
+ * (parallel.f90:2939-3018) and set_grid_derivative / GRID_DERIVATIVE_gcl
+ * (WCNSE5.f90:1478-1728).  dims: 3 ints per block; xyz: 3 pointers per block
+ * (x,y,z); regions: 16 ints per BC region, the integers of the 1976-format BC
+ * file: nb, s_st1,s_ed1,s_st2,s_ed2,s_st3,s_ed3, bctype,
+ * t_st1,t_ed1,t_st2,t_ed2,t_st3,t_ed3, nbt, ibcwin. */
+int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, const double *const *xyz, int nregions,
+                const int *regions, WcnsContext **out);
+void wcns_destroy(WcnsContext *ctx);
+const char *wcns_last_error(void);
+
+/* State transfer (init_nstart0/1, flow-file read/write PostProcess.f90:1387-1396) */
+int wcns_set_prim(WcnsContext *ctx, int nb, const double *r, const double *u, const double *v, const double *w,
+                  const double *p, const double *t);
+int wcns_get_field(WcnsContext *ctx, int field, int nb, double *out);
+int wcns_set_field(WcnsContext *ctx, int field, int nb, const double *in);
+
+/* Per-step drop-ins, in the reference's call order (Main.f90:85-109). */
+int wcns_boundary_all(WcnsContext *ctx);        /* exchange_bc + boundary_all (Main.f90:85-87) */
+int wcns_initial_q_dq_c_t(WcnsContext *ctx);    /* initial_q_dq_c_t (sub_tgh.f90:1-32) */
+int wcns_timestep(WcnsContext *ctx);            /* timestep_tgh (sub_tgh.f90:1270-1348) */
+int wcns_rhs_vis(WcnsContext *ctx);             /* r_h_s_vis (RHS.f90:2-30), laminar */
+int wcns_communicate_dq(WcnsContext *ctx);      /* communicate_dq_npp (parallel.f90:3020-3058) */
+int wcns_rhs_invis(WcnsContext *ctx);           /* r_h_s_invis (RHS.f90:35-72) */
+int wcns_lhs(WcnsContext *ctx);                 /* l_h_s_tgh (LHS.f90:1-34) */
+int wcns_communicate_pv(WcnsContext *ctx);      /* communicate_pv_npp (parallel.f90:3166-3215) */
+int wcns_residual(WcnsContext *ctx, double *res_per_block, double *resmax_per_block, double *rms);
+                                                /* residual_curve (PostProcess.f90:1195-1347) */
+
+/* The whole step of Main.f90:85-109 repeated nsteps times, replayed from a
+ * CUDA graph.  rms_history (may be NULL) receives the residual RMS of every
+ * step. */
+int wcns_step(WcnsContext *ctx, int nsteps, double *rms_history);
+
+/* Asynchronous form for timing: enqueue nsteps graph replays on the
+ * context's stream without waiting; wcns_sync waits and checks errors. */
+int wcns_step_async(WcnsContext *ctx, int nsteps);
+int wcns_sync(WcnsContext *ctx);
+/* The context's CUDA stream (cudaStream_t) for event timing. */
+void *wcns_stream(WcnsContext *ctx);
+/* Number of kernel launches one step issues. */
+int wcns_launches_per_step(WcnsContext *ctx);
+/* Number of points shared by more than two blocks (multi-point sets). */
+int wcns_n_multipoints(WcnsContext *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

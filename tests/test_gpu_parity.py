@@ -1,0 +1,109 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Both sides start from the same seeded inputs.  Phase-by-phase comparisons
+must agree to FP64 round-off: the kernels restate the reference operation
+sequence with fused multiply-add disabled, so most fields are bitwise equal;
+the far-field boundary uses pow(), where CUDA's and glibc's results may differ
+in the last bit, so the bar is a relative error of 1e-12 per field.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import compare_fields, compare_prim_scaled, interior, rel_err
+from wcns_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+TOL_PHASE = 1e-12
+TOL_STEPS = 1e-10
+PRIM = ["r", "u", "v", "w", "p"]
+METRICS = ["kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz", "vol"]
+DQ = ["dq1", "dq2", "dq3", "dq4", "dq5"]
+
+
+def make_pair(case):
+    from oracle.pyoracle import Oracle
+    from wcns_b200.solver import Wcns
+    return Wcns(case), Oracle(case)
+
+
+CASES = {
+    "vortex_sw_4": lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=4, nflux=1),
+    "vortex_roe_41": lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=41, nflux=3),
+    "plate_small": lambda: cases.small_plate_case(),
+    "plate_small_nscheme4_sw": lambda: cases.small_plate_case(nscheme=4, nflux=1),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_metrics_bitwise(name):
+    g, o = make_pair(CASES[name]())
+    errs = compare_fields(g, o, METRICS)
+    assert max(errs.values()) == 0.0, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_phase_by_phase(name):
+    case = CASES[name]()
+    g, o = make_pair(case)
+    report = {}
+
+    def cmp(tag, names, region="interior", tol=TOL_PHASE):
+        e = compare_fields(g, o, names, region=region)
+        report[tag] = e
+        assert max(e.values()) <= tol, (tag, e)
+
+    for step in range(2):
+        g.boundary_all(); o.phase("boundary_all")
+        cmp(f"{step}:bc", PRIM, region="all")
+        g.initial_q_dq_c_t(); o.phase("initial_q_dq_c_t")
+        if case.params.nvis == 1:
+            cmp(f"{step}:t", ["t"], region="all")
+        g.timestep_tgh(); o.phase("timestep")
+        cmp(f"{step}:dt", ["dtdt", "sra", "srb", "src", "srva", "srvb", "srvc"])
+        if case.params.nvis == 1:
+            g.r_h_s_vis(); o.phase("rhs_vis")
+            cmp(f"{step}:vis", DQ)
+            g.communicate_dq_npp(); o.phase("communicate_dq")
+            cmp(f"{step}:cdq1", DQ)
+        g.r_h_s_invis(); o.phase("rhs_invis")
+        cmp(f"{step}:inv", DQ)
+        g.communicate_dq_npp(); o.phase("communicate_dq")
+        cmp(f"{step}:cdq2", DQ)
+        g.l_h_s_tgh(); o.phase("lhs")
+        cmp(f"{step}:lhs_dq", DQ)
+        cmp(f"{step}:lhs_prim", PRIM)
+        g.communicate_pv_npp(); o.phase("communicate_pv")
+        cmp(f"{step}:cpv", PRIM + (["t"] if case.params.nvis == 1 else []))
+        res_g = g.residual_curve()
+        res_o = o.residual()
+        assert rel_err(res_g[0], res_o[0]) <= 1e-12
+        assert rel_err(res_g[1], res_o[1]) <= 1e-12
+        assert abs(res_g[2] - res_o[2]) <= 1e-12 * abs(res_o[2])
+    print(name, {k: max(v.values()) for k, v in report.items()})
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_multistep_graph(name):
+    case = CASES[name]()
+    g, o = make_pair(case)
+    n = 20
+    hg = g.step(n)
+    ho = o.step(n)
+    assert np.max(np.abs(hg - ho) / np.abs(ho)) <= TOL_STEPS, (hg, ho)
+    errs = compare_prim_scaled(g, o)
+    print(name, "20 steps", errs, "rms", hg[-1])
+    assert max(errs.values()) <= TOL_STEPS, errs
+
+
+def test_graph_step_equals_phase_calls():
+    case = cases.small_plate_case()
+    from wcns_b200.solver import Wcns
+    a, b = Wcns(case), Wcns(case)
+    a.step(3)
+    for _ in range(3):
+        b.boundary_all(); b.initial_q_dq_c_t(); b.timestep_tgh(); b.r_h_s_vis(); b.communicate_dq_npp()
+        b.r_h_s_invis(); b.communicate_dq_npp(); b.l_h_s_tgh(); b.communicate_pv_npp()
+    for nb in range(1, case.nblocks + 1):
+        for f in PRIM:
+            assert np.array_equal(interior(a.get(f, nb), case.dims[nb - 1]), interior(b.get(f, nb), case.dims[nb - 1]))

@@ -1,0 +1,729 @@
+// capi.cu -- C ABI and host-side set-up of the WCNS B200 path.
+//
+// Host work done once per context (the reference's pre-processing):
+//   * BC regions: analyze_bc / analyze_bc_connect (parallel.f90:1123-1300)
+//     give the face ranges, outward directions and interface image maps;
+//     set_bc_index (PreProcess.f90:2543-2572) orders regions -1,4,5,6,2,3.
+//   * multi-point interface sets: connect_pre_parallel and comp_list_insert
+//     (parallel.f90:177-393, 4202-4311), build_nppos_list_ex (2939-3018).
+//   * device tables: interface ghost-copy list, physical regions per block,
+//     dq-zero list, interface point snapshot list, averaging pairs, line
+//     groups for the residual kernels.
+// Semantics are those of the reference run with one block per MPI rank:
+// exchanges between different blocks use start-of-exchange snapshots; a
+// block connected to itself uses the in-place same-rank path.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/wcns_b200.h"
+#include "wcns_dev.cuh"
+#include "wcns_launch.h"
+
+using namespace wcns;
+
+static thread_local std::string g_err;
+static void set_err(const std::string &s) { g_err = s; }
+extern "C" const char *wcns_last_error(void) { return g_err.c_str(); }
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            set_err(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call);      \
+            return WCNS_ERR_CUDA;                                                              \
+        }                                                                                      \
+    } while (0)
+
+namespace {
+
+struct HReg {
+    int bctype = 0;
+    int raw_s_st[3], raw_s_ed[3], raw_t_st[3], raw_t_ed[3];
+    int nbt = 0, ibcwin = 0;
+    int s_st[3], s_ed[3], s_nd = 0, s_lr = 0, s_lr3d[3];
+    int t_st[3], t_ed[3], t_nd = 0, t_lr = 0, t_lr3d[3];
+    std::vector<int> img[3];
+    int iused = 0;
+    int box(int i, int j, int k) const {
+        int nx = s_ed[0] - s_st[0] + 1, ny = s_ed[1] - s_st[1] + 1;
+        return (i - s_st[0]) + nx * ((j - s_st[1]) + ny * (k - s_st[2]));
+    }
+};
+
+struct HBlock {
+    DevBlock d;
+    std::vector<HReg> regs;
+    std::vector<int> bcindex;
+};
+
+template <class T>
+T *dev_upload(const std::vector<T> &v) {
+    if (v.empty()) return nullptr;
+    T *p = nullptr;
+    if (cudaMalloc(&p, sizeof(T) * v.size()) != cudaSuccess) return nullptr;
+    cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return p;
+}
+
+}  // namespace
+
+struct WcnsContext {
+    WcnsParams prm{};
+    DevParams P{};
+    DevFields F{};
+    std::vector<HBlock> blk;  // 0-based
+    long long total = 0;      // ghosted points over all blocks
+    double *pool = nullptr;
+    cudaStream_t stream = nullptr;
+    LaunchCtx L;
+    std::vector<void *> owned;  // device allocations to free
+    int *d_err = nullptr;
+    double *d_hist = nullptr;
+    int hist_cap = 0;
+    cudaGraphExec_t graph = nullptr;
+    int nmulti = 0;
+    int launches = 0;
+    ~WcnsContext() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void *p : owned) cudaFree(p);
+        if (pool) cudaFree(pool);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    template <class T>
+    T *up(const std::vector<T> &v) {
+        T *p = dev_upload(v);
+        if (p) owned.push_back(p);
+        return p;
+    }
+    long long gi(int nb1, int i, int j, int k) const { return gidx(blk[nb1 - 1].d, i, j, k); }
+};
+
+// ---------------------------------------------------------------------------
+// analyze_bc + analyze_bc_connect (parallel.f90:1123-1300)
+static int analyze(WcnsContext *c) {
+    const int nbk = (int)c->blk.size();
+    for (int b = 0; b < nbk; b++) {
+        HBlock &B = c->blk[b];
+        int dims[3] = {B.d.ni, B.d.nj, B.d.nk};
+        for (HReg &R : B.regs) {
+            for (int m = 0; m < 3; m++) {
+                int a = std::abs(R.raw_s_st[m]), e = std::abs(R.raw_s_ed[m]);
+                R.s_st[m] = std::min(a, e);
+                R.s_ed[m] = std::max(a, e);
+                R.s_lr3d[m] = 0;
+                if (R.raw_s_st[m] == R.raw_s_ed[m]) {
+                    R.s_nd = m + 1;
+                    R.s_lr = R.raw_s_st[m] == 1 ? -1 : 1;
+                    R.s_lr3d[m] = R.s_lr;
+                }
+                if (R.s_st[m] < 1 || R.s_ed[m] > dims[m]) {
+                    set_err("BC region outside its block (block " + std::to_string(b + 1) + ")");
+                    return WCNS_ERR_ARGUMENT;
+                }
+            }
+            if (R.s_nd == 0) { set_err("BC region is not a face"); return WCNS_ERR_ARGUMENT; }
+            if (R.bctype < 0) {
+                if (R.nbt < 1 || R.nbt > nbk) { set_err("interface target block out of range"); return WCNS_ERR_ARGUMENT; }
+                int std_[3][3] = {{0}};
+                for (int m = 0; m < 3; m++) {
+                    R.t_lr3d[m] = 0;
+                    if (R.raw_t_st[m] == R.raw_t_ed[m]) {
+                        R.t_nd = m + 1;
+                        R.t_lr = R.raw_t_st[m] == 1 ? -1 : 1;
+                        R.t_lr3d[m] = R.t_lr;
+                    }
+                }
+                if (R.t_nd == 0) { set_err("interface target is not a face"); return WCNS_ERR_ARGUMENT; }
+                bool done = false;
+                for (int m = 1; m <= 3 && !done; m++)
+                    for (int n = 1; n <= 3 && !done; n++) {
+                        if (m == R.s_nd || n == R.t_nd) continue;
+                        int js1 = R.raw_s_st[m - 1];
+                        if (std::abs(js1) < std::abs(R.raw_s_ed[m - 1])) js1 = R.raw_s_ed[m - 1];
+                        int js2 = R.raw_t_st[n - 1];
+                        if (std::abs(js2) < std::abs(R.raw_t_ed[n - 1])) js2 = R.raw_t_ed[n - 1];
+                        if ((long long)js1 * js2 > 0) {
+                            std_[n - 1][m - 1] = 1;
+                            std_[R.t_nd - 1][R.s_nd - 1] = 1;
+                            std_[6 - n - R.t_nd - 1][6 - m - R.s_nd - 1] = 1;
+                            done = true;
+                        }
+                    }
+                int s_st[3], s_ed[3], t_st[3], s_sign[3], t_sign[3], st_sign[3];
+                for (int m = 0; m < 3; m++) {
+                    s_st[m] = std::abs(R.raw_s_st[m]);
+                    s_ed[m] = std::abs(R.raw_s_ed[m]);
+                    t_st[m] = std::abs(R.raw_t_st[m]);
+                    int t_ed = std::abs(R.raw_t_ed[m]);
+                    s_sign[m] = (m + 1 != R.s_nd && s_st[m] > s_ed[m]) ? -1 : 1;
+                    t_sign[m] = (m + 1 != R.t_nd && t_st[m] > t_ed) ? -1 : 1;
+                    R.t_st[m] = std::min(t_st[m], t_ed);
+                    R.t_ed[m] = std::max(t_st[m], t_ed);
+                }
+                for (int m = 0; m < 3; m++) {
+                    int co = 0;
+                    for (int n = 0; n < 3; n++)
+                        if (std_[n][m]) co = n + 1;
+                    if (!co) { set_err("interface orientation could not be resolved"); return WCNS_ERR_ARGUMENT; }
+                    st_sign[m] = t_sign[co - 1] * s_sign[m];
+                }
+                int nbox = (R.s_ed[0] - R.s_st[0] + 1) * (R.s_ed[1] - R.s_st[1] + 1) * (R.s_ed[2] - R.s_st[2] + 1);
+                for (int q = 0; q < 3; q++) R.img[q].assign(nbox, 0);
+                for (int i = s_st[0];; i += s_sign[0]) {
+                    int id_ = (i - s_st[0]) * st_sign[0];
+                    for (int j = s_st[1];; j += s_sign[1]) {
+                        int jd = (j - s_st[1]) * st_sign[1];
+                        for (int k = s_st[2];; k += s_sign[2]) {
+                            int kd = (k - s_st[2]) * st_sign[2];
+                            int bx = R.box(i, j, k);
+                            for (int q = 0; q < 3; q++) R.img[q][bx] = t_st[q] + std_[q][0] * id_ + std_[q][1] * jd + std_[q][2] * kd;
+                            if (k == s_ed[2]) break;
+                        }
+                        if (j == s_ed[1]) break;
+                    }
+                    if (i == s_ed[0]) break;
+                }
+                const HBlock &T = c->blk[R.nbt - 1];
+                int tdims[3] = {T.d.ni, T.d.nj, T.d.nk};
+                for (int bx = 0; bx < nbox; bx++)
+                    for (int q = 0; q < 3; q++) {
+                        int v = R.img[q][bx];
+                        int lo = q + 1 == R.t_nd ? (R.t_lr < 0 ? 1 : tdims[q]) : 1;
+                        if (v < lo || v > tdims[q] || (q + 1 == R.t_nd && v != lo)) {
+                            set_err("interface image outside the target face");
+                            return WCNS_ERR_ARGUMENT;
+                        }
+                    }
+                if (dims[R.s_nd - 1] < 4 || tdims[R.t_nd - 1] < 4) {
+                    set_err("interface needs at least 4 points normal to the face");
+                    return WCNS_ERR_ARGUMENT;
+                }
+            } else if (R.bctype < 2 || R.bctype > 6) {
+                set_err("unsupported BC type " + std::to_string(R.bctype) + " (supported: -1,2,3,4,5,6)");
+                return WCNS_ERR_UNSUPPORTED;
+            }
+        }
+        static const int order[6] = {-1, 4, 5, 6, 2, 3};
+        B.bcindex.clear();
+        for (int l = 0; l < 6; l++)
+            for (int r = 0; r < (int)B.regs.size(); r++) {
+                int t = B.regs[r].bctype < 0 ? -1 : B.regs[r].bctype;
+                if (t == order[l]) B.bcindex.push_back(r);
+            }
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+static int build_tables(WcnsContext *c) {
+    const int nbk = (int)c->blk.size();
+    LaunchCtx &L = c->L;
+    // interface ghost copies
+    std::vector<GhostCopy> ghost;
+    for (int b = 0; b < nbk; b++)
+        for (const HReg &R : c->blk[b].regs) {
+            if (R.bctype >= 0) continue;
+            for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                    for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                        int bx = R.box(i, j, k);
+                        for (int l = 1; l <= 3; l++) {
+                            GhostCopy g;
+                            g.dst = c->gi(b + 1, i + l * R.s_lr3d[0], j + l * R.s_lr3d[1], k + l * R.s_lr3d[2]);
+                            g.src = c->gi(R.nbt, R.img[0][bx] - l * R.t_lr3d[0], R.img[1][bx] - l * R.t_lr3d[1],
+                                          R.img[2][bx] - l * R.t_lr3d[2]);
+                            ghost.push_back(g);
+                        }
+                    }
+        }
+    L.nghost = (long long)ghost.size();
+    L.ghost = c->up(ghost);
+    // physical regions in bcindex order, dq-zero points
+    std::vector<DevRegion> regs;
+    std::vector<int> first(nbk + 1, 0);
+    std::vector<long long> zero;
+    for (int b = 0; b < nbk; b++) {
+        first[b] = (int)regs.size();
+        for (int r : c->blk[b].bcindex) {
+            const HReg &R = c->blk[b].regs[r];
+            if (R.bctype < 0) continue;
+            DevRegion d{};
+            d.blk = b;
+            d.bctype = R.bctype;
+            for (int m = 0; m < 3; m++) { d.s_st[m] = R.s_st[m]; d.s_ed[m] = R.s_ed[m]; d.s_lr3d[m] = R.s_lr3d[m]; }
+            d.s_nd = R.s_nd;
+            d.s_lr = R.s_lr;
+            regs.push_back(d);
+        }
+        for (const HReg &R : c->blk[b].regs) {
+            if (R.bctype <= 0) continue;
+            for (int i = R.s_st[0]; i <= R.s_ed[0]; i++)
+                for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                    for (int k = R.s_st[2]; k <= R.s_ed[2]; k++) zero.push_back(c->gi(b + 1, i, j, k));
+        }
+    }
+    first[nbk] = (int)regs.size();
+    L.regions = c->up(regs);
+    L.reg_first = c->up(first);
+    L.nzero = (long long)zero.size();
+    L.zero_pts = c->up(zero);
+    // interface averaging: snapshot slots, pairs per region (region order)
+    std::unordered_map<long long, int> slot;
+    std::vector<long long> snap_pts;
+    auto slot_of = [&](long long id) {
+        auto it = slot.find(id);
+        if (it != slot.end()) return it->second;
+        int s = (int)snap_pts.size();
+        slot[id] = s;
+        snap_pts.push_back(id);
+        return s;
+    };
+    std::vector<PairEntry> pairs;
+    std::vector<int> reg_pair_first, blk_reg_first(nbk + 1, 0);
+    for (int b = 0; b < nbk; b++) {
+        blk_reg_first[b] = (int)reg_pair_first.size();
+        for (const HReg &R : c->blk[b].regs) {
+            if (R.bctype >= 0) continue;
+            reg_pair_first.push_back((int)pairs.size());
+            for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                    for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                        int bx = R.box(i, j, k);
+                        PairEntry e;
+                        e.own = c->gi(b + 1, i, j, k);
+                        e.partner = c->gi(R.nbt, R.img[0][bx], R.img[1][bx], R.img[2][bx]);
+                        slot_of(e.own);
+                        e.partner_slot = slot_of(e.partner);
+                        e.same = (R.nbt == b + 1) ? 1 : 0;
+                        pairs.push_back(e);
+                    }
+        }
+    }
+    blk_reg_first[nbk] = (int)reg_pair_first.size();
+    reg_pair_first.push_back((int)pairs.size());
+    L.nsnap = (int)snap_pts.size();
+    L.snap_pts = c->up(snap_pts);
+    L.pairs = c->up(pairs);
+    L.reg_pair_first = c->up(reg_pair_first);
+    L.blk_reg_first = c->up(blk_reg_first);
+    if (L.nsnap) {
+        CK(cudaMalloc(&L.snap, sizeof(double) * 6 * L.nsnap));
+        c->owned.push_back(L.snap);
+    }
+    // multi-point sets: connect_pre_parallel + comp_list_insert
+    for (auto &B : c->blk)
+        for (auto &R : B.regs) R.iused = 0;
+    for (int b = 0; b < nbk; b++)
+        for (auto &R : c->blk[b].regs) {
+            if (R.bctype < 0 && R.iused == 0) {
+                R.iused = 1;
+                HBlock &T = c->blk[R.nbt - 1];
+                if (R.ibcwin >= 1 && R.ibcwin <= (int)T.regs.size()) T.regs[R.ibcwin - 1].iused = -1;
+            }
+        }
+    std::vector<std::vector<long long>> comps;  // members as field indices, list order
+    for (int b = 0; b < nbk; b++)
+        for (auto &R : c->blk[b].regs) {
+            if (R.bctype >= 0 || R.iused != 1) continue;
+            static const int mcyc[5] = {1, 2, 3, 1, 2};
+            int d2 = mcyc[R.s_nd] - 1, d3 = mcyc[R.s_nd + 1] - 1;
+            for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                    for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                        int cc[3] = {i, j, k};
+                        bool inner = cc[d2] >= R.s_st[d2] + 1 && cc[d2] <= R.s_ed[d2] - 1 && cc[d3] >= R.s_st[d3] + 1 &&
+                                     cc[d3] <= R.s_ed[d3] - 1;
+                        if (inner) continue;
+                        int bx = R.box(i, j, k);
+                        long long a = c->gi(b + 1, i, j, k);
+                        long long t = c->gi(R.nbt, R.img[0][bx], R.img[1][bx], R.img[2][bx]);
+                        bool ok = false;
+                        for (auto &cl : comps) {
+                            bool ea = std::find(cl.begin(), cl.end(), a) != cl.end();
+                            bool et = std::find(cl.begin(), cl.end(), t) != cl.end();
+                            if (ea || et) {
+                                if (!ea) cl.push_back(a);
+                                if (!et) cl.push_back(t);
+                                ok = true;
+                                break;
+                            }
+                        }
+                        if (!ok) comps.push_back({a, t});
+                    }
+        }
+    std::vector<int> comp_first, comp_n, mem_slot, mem_comp;
+    std::vector<long long> mem_idx;
+    for (auto &cl : comps) {
+        if (cl.size() <= 2) continue;
+        int cid = (int)comp_first.size();
+        comp_first.push_back((int)mem_idx.size());
+        comp_n.push_back((int)cl.size());
+        for (long long id : cl) {
+            mem_idx.push_back(id);
+            mem_slot.push_back(slot_of(id));
+            mem_comp.push_back(cid);
+        }
+    }
+    if ((int)snap_pts.size() != L.nsnap) { set_err("internal: snapshot list grew"); return WCNS_ERR_ARGUMENT; }
+    c->nmulti = (int)comp_first.size();
+    L.ncomp = (int)comp_first.size();
+    L.nmem = (int)mem_idx.size();
+    L.comp_first = c->up(comp_first);
+    L.comp_n = c->up(comp_n);
+    L.mem_slot = c->up(mem_slot);
+    L.mem_comp = c->up(mem_comp);
+    L.mem_idx = c->up(mem_idx);
+    // line groups for the residual kernels
+    size_t inv_smem = 0, vis_smem = 0;
+    for (int dir = 0; dir < 3; dir++) {
+        for (int pass = 0; pass < 2; pass++) {  // 0 inviscid, 1 viscous
+            std::vector<LineGroup> g;
+            int nl_max = 0, hmax = 0;
+            for (int b = 0; b < nbk; b++) {
+                const DevBlock &D = c->blk[b].d;
+                int n = dimof(D, dir);
+                if (pass == 0 && n <= NIJK2D) continue;
+                int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
+                int na = dimof(D, a1), nb2 = dimof(D, a2);
+                int NL = std::max(1, std::min(8, 512 / (n + 1)));
+                for (int bb = 1; bb <= nb2; bb++)
+                    for (int a = 1; a <= na; a += NL) {
+                        LineGroup lg{b, a, bb, std::min(NL, na - a + 1)};
+                        g.push_back(lg);
+                        nl_max = std::max(nl_max, lg.nl);
+                    }
+                hmax = std::max(hmax, n + 1);
+            }
+            DirTable &T = pass == 0 ? L.inv[dir] : L.vis[dir];
+            T.ngroups = (int)g.size();
+            T.nl_max = nl_max;
+            T.hmax = hmax;
+            T.groups = c->up(g);
+            size_t sm = pass == 0 ? (size_t)nl_max * (15 * (size_t)hmax + 130) * 8 : (size_t)nl_max * 5 * (size_t)hmax * 8;
+            if (pass == 0) inv_smem = std::max(inv_smem, sm);
+            else vis_smem = std::max(vis_smem, sm);
+        }
+    }
+    if (inv_smem > 227 * 1024 || vis_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
+    setup_rhs_invis_attrs(std::max<size_t>(inv_smem, 48 * 1024));
+    setup_rhs_vis_attrs(std::max<size_t>(vis_smem, 48 * 1024));
+    // residual partials, update bad lists
+    L.res_ctas_per_block = 32;
+    CK(cudaMalloc(&L.res_partial, sizeof(double) * 2 * 32 * nbk));
+    c->owned.push_back(L.res_partial);
+    CK(cudaMalloc(&L.res_out, sizeof(double) * (2 * nbk + 1)));
+    c->owned.push_back(L.res_out);
+    CK(cudaMalloc(&L.bad_count, sizeof(int) * nbk));
+    c->owned.push_back(L.bad_count);
+    CK(cudaMemset(L.bad_count, 0, sizeof(int) * nbk));
+    CK(cudaMalloc(&L.bad_list, sizeof(long long) * BAD_CAP * nbk));
+    c->owned.push_back(L.bad_list);
+    return 0;
+}
+
+static int check_errors(WcnsContext *c) {
+    int h[ERR_NSLOTS];
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(h, c->d_err, sizeof h, cudaMemcpyDeviceToHost));
+    CK(cudaMemset(c->d_err, 0, sizeof h));
+    if (h[ERR_ROE]) { set_err("flux_Roe: c^2 <= 0 at " + std::to_string(h[ERR_ROE]) + " half nodes"); return WCNS_ERR_ROE; }
+    if (h[ERR_UPDATE_BLOCKS]) { set_err("update_limited: too many non-physical points"); return WCNS_ERR_UPDATE; }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, const double *const *xyz, int nregions,
+                           const int *regions, WcnsContext **out) {
+    if (!prm || nblocks < 1 || !dims || !xyz || !out || (nregions > 0 && !regions)) {
+        set_err("wcns_create: invalid argument");
+        return WCNS_ERR_ARGUMENT;
+    }
+    if (prm->nscheme != 4 && prm->nscheme != 41) { set_err("nscheme must be 4 or 41"); return WCNS_ERR_UNSUPPORTED; }
+    if (prm->nflux != 1 && prm->nflux != 3) { set_err("nflux must be 1 (Steger-Warming) or 3 (Roe)"); return WCNS_ERR_UNSUPPORTED; }
+    if (prm->nvis != 0 && prm->nvis != 1) { set_err("nvis must be 0 or 1"); return WCNS_ERR_ARGUMENT; }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_err("no CUDA device"); return WCNS_ERR_CUDA; }
+    WcnsContext *c = new WcnsContext();
+    c->prm = *prm;
+    // derived constants (init_inflow PreProcess.f90:968-1113; read_perfect_gasmodel GasModel.f90:184-217)
+    const double PAI = 3.14159265;
+    DevParams &P = c->P;
+    P.gama = 1.40;
+    P.g1 = P.gama / (P.gama - 1.0);
+    P.moo = prm->moo;
+    P.moo2 = prm->moo * prm->moo;
+    P.moocp = prm->moo * prm->moo * P.gama;
+    P.reynolds = (prm->reynolds / 1.0) * 1.0;
+    P.re = 1.0 / P.reynolds;
+    P.visc = 110.4 / prm->tref;
+    double cp = 1.0 / ((P.gama - 1.0) * prm->moo * prm->moo);
+    P.cp_prl = cp / 0.72;
+    P.cp_prt = cp / 0.90;
+    P.cc23 = 2.0 / 3.0;
+    P.cfl = prm->cfl;
+    P.timedt_rate = prm->timedt_rate;
+    P.efix = prm->efix;
+    P.csrv = prm->csrv;
+    double attack = prm->attack * PAI / 180.0, sideslip = prm->sideslip * PAI / 180.0;
+    P.uoo = cos(attack) * cos(sideslip);
+    P.voo = sin(attack) * cos(sideslip);
+    P.woo = sin(sideslip);
+    P.roo = 1.0;
+    P.poo = 1.0 / (P.gama * prm->moo * prm->moo);
+    P.coo = sqrt(P.gama * P.poo / P.roo);
+    P.twall_nd = prm->twall / prm->tref;
+    P.nvis = prm->nvis;
+    P.nscheme = prm->nscheme;
+    P.nflux = prm->nflux;
+    P.adiabatic = prm->twall > 0.0 ? 0 : 1;
+    // blocks
+    c->blk.resize(nblocks);
+    long long off = 0;
+    for (int b = 0; b < nblocks; b++) {
+        DevBlock &d = c->blk[b].d;
+        d.ni = dims[3 * b];
+        d.nj = dims[3 * b + 1];
+        d.nk = dims[3 * b + 2];
+        if (d.ni < 2 || d.nj < 2 || d.nk < 2) { delete c; set_err("block dimensions must be >= 2"); return WCNS_ERR_ARGUMENT; }
+        d.gx = d.ni + 6;
+        d.gy = d.nj + 6;
+        d.gz = d.nk + 6;
+        d.off = off;
+        d.npts = (long long)d.ni * d.nj * d.nk;
+        off += (long long)d.gx * d.gy * d.gz;
+        off = (off + 31) / 32 * 32;
+    }
+    c->total = off;
+    for (int r = 0; r < nregions; r++) {
+        const int *rr = regions + 16 * r;
+        if (rr[0] < 1 || rr[0] > nblocks) { delete c; set_err("BC region block number out of range"); return WCNS_ERR_ARGUMENT; }
+        HReg R;
+        for (int m = 0; m < 3; m++) {
+            R.raw_s_st[m] = rr[1 + 2 * m];
+            R.raw_s_ed[m] = rr[2 + 2 * m];
+            R.raw_t_st[m] = rr[8 + 2 * m];
+            R.raw_t_ed[m] = rr[9 + 2 * m];
+        }
+        R.bctype = rr[7];
+        R.nbt = rr[14];
+        R.ibcwin = rr[15];
+        c->blk[rr[0] - 1].regs.push_back(R);
+    }
+    int rc = analyze(c);
+    if (rc) { delete c; return rc; }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        set_err("cudaStreamCreate failed");
+        return WCNS_ERR_CUDA;
+    }
+    // field pool
+    size_t bytes = sizeof(double) * (size_t)F_NALL * (size_t)c->total;
+    if (cudaMalloc(&c->pool, bytes) != cudaSuccess) { delete c; set_err("device allocation of the field pool failed"); return WCNS_ERR_CUDA; }
+    cudaMemset(c->pool, 0, bytes);
+    for (int f = 0; f < F_NALL; f++) c->F.f[f] = c->pool + (size_t)f * c->total;
+    std::vector<DevBlock> hb(nblocks);
+    for (int b = 0; b < nblocks; b++) hb[b] = c->blk[b].d;
+    LaunchCtx &L = c->L;
+    L.stream = c->stream;
+    L.P = &c->P;
+    L.F = &c->F;
+    L.nblocks = nblocks;
+    L.blocks = c->up(hb);
+    rc = build_tables(c);
+    if (rc) { delete c; return rc; }
+    CK(cudaMalloc(&c->d_err, sizeof(int) * ERR_NSLOTS));
+    c->owned.push_back(c->d_err);
+    CK(cudaMemset(c->d_err, 0, sizeof(int) * ERR_NSLOTS));
+    L.err = c->d_err;
+    // host block table the launchers read
+    auto *hbl = new DevBlock[nblocks];
+    for (int b = 0; b < nblocks; b++) hbl[b] = hb[b];
+    L.hblocks = hbl;
+    // grid metrics on the device
+    double *xyzd = nullptr, *work = nullptr;
+    CK(cudaMalloc(&xyzd, sizeof(double) * 3 * (size_t)c->total));
+    CK(cudaMalloc(&work, sizeof(double) * 13 * (size_t)c->total));
+    cudaMemset(xyzd, 0, sizeof(double) * 3 * (size_t)c->total);
+    std::vector<double> tmp;
+    for (int b = 0; b < nblocks; b++) {
+        const DevBlock &d = hb[b];
+        tmp.assign((size_t)d.gx * d.gy * d.gz, 0.0);
+        for (int q = 0; q < 3; q++) {
+            const double *src = xyz[3 * b + q];
+            if (!src) { set_err("missing coordinates"); cudaFree(xyzd); cudaFree(work); delete c; return WCNS_ERR_ARGUMENT; }
+            for (int k = 1; k <= d.nk; k++)
+                for (int j = 1; j <= d.nj; j++)
+                    for (int i = 1; i <= d.ni; i++)
+                        tmp[gidx(d, i, j, k) - d.off] = src[(i - 1) + (size_t)d.ni * ((j - 1) + (size_t)d.nj * (k - 1))];
+            cudaMemcpy(xyzd + (size_t)q * c->total + d.off, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice);
+        }
+    }
+    double *xyzp[3] = {xyzd, xyzd + c->total, xyzd + 2 * c->total};
+    launch_metrics(L, xyzp, work);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(xyzd);
+    cudaFree(work);
+    if (e != cudaSuccess) { set_err(std::string("metrics: ") + cudaGetErrorString(e)); delete c; return WCNS_ERR_CUDA; }
+    *out = c;
+    return 0;
+}
+
+extern "C" void wcns_destroy(WcnsContext *c) {
+    if (!c) return;
+    cudaStreamSynchronize(c->stream);
+    delete[] c->L.hblocks;
+    delete c;
+}
+
+static int block_range(WcnsContext *c, int nb, const DevBlock **d) {
+    if (!c || nb < 1 || nb > (int)c->blk.size()) { set_err("block number out of range"); return WCNS_ERR_ARGUMENT; }
+    *d = &c->blk[nb - 1].d;
+    return 0;
+}
+
+extern "C" int wcns_set_prim(WcnsContext *c, int nb, const double *r, const double *u, const double *v, const double *w,
+                             const double *p, const double *t) {
+    const DevBlock *d;
+    if (int rc = block_range(c, nb, &d)) return rc;
+    const double *src[6] = {r, u, v, w, p, t};
+    size_t n = (size_t)d->gx * d->gy * d->gz;
+    for (int f = 0; f < 6; f++) {
+        if (!src[f]) { set_err("wcns_set_prim: null array"); return WCNS_ERR_ARGUMENT; }
+        CK(cudaMemcpyAsync(c->F.f[F_R + f] + d->off, src[f], sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_get_field(WcnsContext *c, int field, int nb, double *out) {
+    const DevBlock *d;
+    if (int rc = block_range(c, nb, &d)) return rc;
+    if (field < 0 || field > WCNS_F_VOL || !out) { set_err("wcns_get_field: unsupported field"); return WCNS_ERR_UNSUPPORTED; }
+    size_t n = (size_t)d->gx * d->gy * d->gz;
+    CK(cudaMemcpyAsync(out, c->F.f[field] + d->off, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_set_field(WcnsContext *c, int field, int nb, const double *in) {
+    const DevBlock *d;
+    if (int rc = block_range(c, nb, &d)) return rc;
+    if (field < 0 || field > WCNS_F_VOL || !in) { set_err("wcns_set_field: unsupported field"); return WCNS_ERR_UNSUPPORTED; }
+    size_t n = (size_t)d->gx * d->gy * d->gz;
+    CK(cudaMemcpyAsync(c->F.f[field] + d->off, in, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+#define PHASE(name, body)                                              \
+    extern "C" int name(WcnsContext *c) {                              \
+        if (!c) { set_err(#name ": null context"); return WCNS_ERR_ARGUMENT; } \
+        body;                                                          \
+        CK(cudaGetLastError());                                        \
+        return check_errors(c);                                        \
+    }
+
+PHASE(wcns_boundary_all, launch_boundary(c->L))
+PHASE(wcns_initial_q_dq_c_t, launch_init(c->L))
+PHASE(wcns_timestep, launch_timestep(c->L))
+PHASE(wcns_rhs_vis, if (c->P.nvis == 1) {
+    launch_node_derivatives(c->L);
+    for (int d = 0; d < 3; d++) launch_rhs_vis(c->L, d);
+})
+PHASE(wcns_communicate_dq, launch_communicate(c->L, 0))
+PHASE(wcns_rhs_invis, for (int d = 0; d < 3; d++) launch_rhs_invis(c->L, d))
+PHASE(wcns_lhs, {
+    launch_lhs(c->L);
+    launch_update(c->L);
+})
+PHASE(wcns_communicate_pv, launch_communicate(c->L, 1))
+
+extern "C" int wcns_residual(WcnsContext *c, double *res, double *resmax, double *rms) {
+    if (!c) { set_err("null context"); return WCNS_ERR_ARGUMENT; }
+    launch_residual(c->L, nullptr);
+    CK(cudaGetLastError());
+    int nb = (int)c->blk.size();
+    std::vector<double> h(2 * nb + 1);
+    CK(cudaMemcpyAsync(h.data(), c->L.res_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (res) std::copy(h.begin(), h.begin() + nb, res);
+    if (resmax) std::copy(h.begin() + nb, h.begin() + 2 * nb, resmax);
+    if (rms) *rms = h[2 * nb];
+    return 0;
+}
+
+// one complete step (Main.f90:85-109) on the context stream
+static int enqueue_step(WcnsContext *c, double *rms_slot) {
+    LaunchCtx &L = c->L;
+    int n = 0;
+    launch_boundary(L); n += 2;
+    launch_init(L); n += 1;
+    launch_timestep(L); n += 1;
+    if (c->P.nvis == 1) {
+        launch_node_derivatives(L); n += 1;
+        for (int d = 0; d < 3; d++) { launch_rhs_vis(L, d); n += L.vis[d].ngroups ? 1 : 0; }
+        launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
+    }
+    for (int d = 0; d < 3; d++) { launch_rhs_invis(L, d); n += L.inv[d].ngroups ? 1 : 0; }
+    launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
+    launch_lhs(L); n += 4 + (L.nzero ? 2 : 0);
+    launch_update(L); n += 2;
+    launch_communicate(L, 1); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
+    launch_residual(L, rms_slot); n += 2;
+    c->launches = n;
+    CK(cudaGetLastError());
+    return 0;
+}
+
+static int build_graph(WcnsContext *c) {
+    if (c->graph) return 0;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(c, nullptr);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) { set_err(std::string("graph capture: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { set_err(std::string("graph instantiate: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
+    return 0;
+}
+
+extern "C" int wcns_step_async(WcnsContext *c, int nsteps) {
+    if (!c || nsteps < 0) { set_err("wcns_step_async: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = build_graph(c)) return rc;
+    for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->graph, c->stream));
+    return 0;
+}
+
+extern "C" int wcns_sync(WcnsContext *c) {
+    if (!c) return WCNS_ERR_ARGUMENT;
+    return check_errors(c);
+}
+
+extern "C" int wcns_step(WcnsContext *c, int nsteps, double *rms_history) {
+    if (!c || nsteps < 0) { set_err("wcns_step: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = build_graph(c)) return rc;
+    int nb = (int)c->blk.size();
+    for (int s = 0; s < nsteps; s++) {
+        CK(cudaGraphLaunch(c->graph, c->stream));
+        if (rms_history) CK(cudaMemcpyAsync(rms_history + s, c->L.res_out + 2 * nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    return check_errors(c);
+}
+
+extern "C" void *wcns_stream(WcnsContext *c) { return c ? (void *)c->stream : nullptr; }
+extern "C" int wcns_launches_per_step(WcnsContext *c) {
+    if (!c) return 0;
+    if (!c->launches) {
+        // count by enqueueing into a throw-away capture
+        build_graph(c);
+    }
+    return c->launches;
+}
+extern "C" int wcns_n_multipoints(WcnsContext *c) { return c ? c->nmulti : 0; }

@@ -1,0 +1,331 @@
+// k_rhs_inv.cu -- inviscid residual along one index direction.
+//
+// Restates r_h_s_invis (RHS.f90:35-72) -> invcode -> inviscd3d
+// (Convect.f90:2-56, 58-649) with the WCNS-E-5 line scheme WCNS_E_5
+// (WCNSE5.f90:2-206, nscheme=4) or WCNS_E_5_41 (WCNSE5.f90:2087-2759,
+// nscheme=41), Steger-Warming (flux.f90:2-77) or Roe (flux.f90:116-244)
+// fluxes, and FLUX_DXYZ (WCNSE5.f90:209-254).  dq += dF.
+//
+// One CTA owns a group of NL lines of one block.  The reference's
+// sequential line loop is split into three parallel phases:
+//   A  per point i: smoothness indicators and nonlinear weights, giving the
+//      left state at half node i and the right state at half node i-1;
+//   B  per half node: boundary closures, positivity fallback, numerical flux;
+//      plus the 26 independent fluxes of the nscheme=41 boundary sections;
+//   C  per point: sixth-order flux difference (or the boundary-section
+//      difference where the reference overrides it) accumulated into dq.
+// Each value is produced with the reference's exact operation sequence.
+#include "wcns_dev.cuh"
+#include "wcns_launch.h"
+
+namespace wcns {
+
+struct InvLine {
+    const double *q[5];  // base pointers (index of point l is (l+2)*stride)
+    long long stride;
+    long long dqbase;    // field index of point l=0 on the line (point l at dqbase + l*stride)
+    int n, ist, ied;
+};
+
+__device__ __forceinline__ double qv(const InvLine &L, int m, int l) { return __ldg(L.q[m] + (long long)(l + 2) * L.stride); }
+
+// qwl/qwr after phase B (main value from smem or the 4-style closure)
+__device__ __forceinline__ double qwl_postB(const InvLine &L, const double *sqwl, int m, int h) {
+    int n = L.n;
+    if (L.ist > 1) {
+        if (h == 0) return (35.0 * qv(L, m, 1) - 35.0 * qv(L, m, 2) + 21.0 * qv(L, m, 3) - 5.0 * qv(L, m, 4)) / 16.0;
+        if (h == 1) return (5.0 * qv(L, m, 1) + 15.0 * qv(L, m, 2) - 5.0 * qv(L, m, 3) + qv(L, m, 4)) / 16.0;
+        if (h == 2) return (-qv(L, m, 1) + 9.0 * qv(L, m, 2) + 9.0 * qv(L, m, 3) - qv(L, m, 4)) / 16.0;
+    }
+    if (L.ied < n) {
+        if (h == n) return (35.0 * qv(L, m, n) - 35.0 * qv(L, m, n - 1) + 21.0 * qv(L, m, n - 2) - 5.0 * qv(L, m, n - 3)) / 16.0;
+        if (h == n - 1) return (5.0 * qv(L, m, n) + 15.0 * qv(L, m, n - 1) - 5.0 * qv(L, m, n - 2) + qv(L, m, n - 3)) / 16.0;
+    }
+    return sqwl[m * (n + 1) + h];
+}
+__device__ __forceinline__ double qwr_postB(const InvLine &L, const double *sqwr, int m, int h) {
+    int n = L.n;
+    if (L.ist > 1) {
+        if (h == 0) return (35.0 * qv(L, m, 1) - 35.0 * qv(L, m, 2) + 21.0 * qv(L, m, 3) - 5.0 * qv(L, m, 4)) / 16.0;
+        if (h == 1) return (5.0 * qv(L, m, 1) + 15.0 * qv(L, m, 2) - 5.0 * qv(L, m, 3) + qv(L, m, 4)) / 16.0;
+    }
+    if (L.ied < n) {
+        if (h == n) return (35.0 * qv(L, m, n) - 35.0 * qv(L, m, n - 1) + 21.0 * qv(L, m, n - 2) - 5.0 * qv(L, m, n - 3)) / 16.0;
+        if (h == n - 1) return (5.0 * qv(L, m, n) + 15.0 * qv(L, m, n - 1) - 5.0 * qv(L, m, n - 2) + qv(L, m, n - 3)) / 16.0;
+        if (h == n - 2) return (-qv(L, m, n) + 9.0 * qv(L, m, n - 1) + 9.0 * qv(L, m, n - 2) - qv(L, m, n - 3)) / 16.0;
+    }
+    return sqwr[m * (n + 1) + h];
+}
+
+// Left boundary-section states (WCNSE5.f90:2284-2459)
+__device__ __forceinline__ double s1_state(const InvLine &L, int m, int h) {
+    switch (h) {
+    case 0: return (3.0 * qv(L, m, 1) - 1.0 * qv(L, m, 2) - 0. * qv(L, m, 3)) / 2.0;
+    case 1: return (19.0 * qv(L, m, 1) + 25.0 * qv(L, m, 2) - 2. * qv(L, m, 3)) / 42.0;
+    case 2: return (4.0 * qv(L, m, 1) + 3.0 * qv(L, m, 2) + 9.0 * qv(L, m, 3) + 2. * qv(L, m, 4)) / 18.0;
+    default: return (-2.0 * qv(L, m, 1) + 3.0 * qv(L, m, 2) + 3.0 * qv(L, m, 3) + 2. * qv(L, m, 4)) / 6.0;
+    }
+}
+__device__ __forceinline__ double s2_left(const InvLine &L, int m, int h) {
+    switch (h) {
+    case 1: return (3.0 * qv(L, m, 1) + 6.0 * qv(L, m, 2) - qv(L, m, 3)) / 8.0;
+    case 2: return (-30.0 * qv(L, m, 1) + 145.0 * qv(L, m, 2) + 29.0 * qv(L, m, 3) - 8.0 * qv(L, m, 4)) / 136.0;
+    case 3: return (-qv(L, m, 2) + 6.0 * qv(L, m, 3) + 3.0 * qv(L, m, 4)) / 8.0;
+    case 4: return (qv(L, m, 2) + 2.0 * qv(L, m, 3) + 5.0 * qv(L, m, 4)) / 8.0;
+    default: return (qv(L, m, 2) + qv(L, m, 3) + 6.0 * qv(L, m, 4)) / 8.0;
+    }
+}
+__device__ __forceinline__ double s2_right(const InvLine &L, int m, int h) {
+    if (h == 2) return (2.0 * qv(L, m, 1) + 49.0 * qv(L, m, 2) + 125.0 * qv(L, m, 3) - 40.0 * qv(L, m, 4)) / 136.0;
+    return s2_left(L, m, h);
+}
+__device__ __forceinline__ double s3_left(const InvLine &L, int m, int h) {
+    if (h == 2) return (-29.0 * qv(L, m, 1) + 170.0 * qv(L, m, 2) + 63.0 * qv(L, m, 3) + 12.0 * qv(L, m, 4)) / 216.0;
+    return s2_left(L, m, h);
+}
+// Right boundary-section states (WCNSE5.f90:2524-2705); h counts down from n
+__device__ __forceinline__ double s4_state(const InvLine &L, int m, int h) {
+    int n = L.n;
+    int o = n - h;
+    switch (o) {
+    case 0: return (3.0 * qv(L, m, n) - 1.0 * qv(L, m, n - 1) - 0. * qv(L, m, n - 2)) / 2.0;
+    case 1: return (19.0 * qv(L, m, n) + 25.0 * qv(L, m, n - 1) - 2. * qv(L, m, n - 2)) / 42.0;
+    case 2: return (4.0 * qv(L, m, n) + 3.0 * qv(L, m, n - 1) + 9.0 * qv(L, m, n - 2) + 2. * qv(L, m, n - 3)) / 18.0;
+    default: return (-2.0 * qv(L, m, n) + 3.0 * qv(L, m, n - 1) + 3.0 * qv(L, m, n - 2) + 2. * qv(L, m, n - 3)) / 6.0;
+    }
+}
+__device__ __forceinline__ double s5_right(const InvLine &L, int m, int h) {
+    int n = L.n;
+    switch (n - h) {
+    case 1: return (3.0 * qv(L, m, n) + 6.0 * qv(L, m, n - 1) - qv(L, m, n - 2)) / 8.0;
+    case 2: return (-30.0 * qv(L, m, n) + 145.0 * qv(L, m, n - 1) + 29.0 * qv(L, m, n - 2) - 8.0 * qv(L, m, n - 3)) / 136.0;
+    case 3: return (-qv(L, m, n - 1) + 6.0 * qv(L, m, n - 2) + 3.0 * qv(L, m, n - 3)) / 8.0;
+    case 4: return (qv(L, m, n - 1) + 2.0 * qv(L, m, n - 2) + 5.0 * qv(L, m, n - 3)) / 8.0;
+    default: return (qv(L, m, n - 1) + qv(L, m, n - 2) + 6.0 * qv(L, m, n - 3)) / 8.0;
+    }
+}
+__device__ __forceinline__ double s5_left(const InvLine &L, int m, int h) {
+    int n = L.n;
+    if (n - h == 2) return (2.0 * qv(L, m, n) + 49.0 * qv(L, m, n - 1) + 125.0 * qv(L, m, n - 2) - 40.0 * qv(L, m, n - 3)) / 136.0;
+    return s5_right(L, m, h);
+}
+__device__ __forceinline__ double s6_right(const InvLine &L, int m, int h) {
+    int n = L.n;
+    if (n - h == 2) return (-29.0 * qv(L, m, n) + 170.0 * qv(L, m, n - 1) + 63.0 * qv(L, m, n - 2) + 12.0 * qv(L, m, n - 3)) / 216.0;
+    return s5_right(L, m, h);
+}
+// qwl(h) at the moment the right sections save u_l_old: the left sections'
+// final values where they ran (h<=5), otherwise the phase-B value.
+__device__ __forceinline__ double qwl_preright(const InvLine &L, const double *sqwl, int nscheme, int m, int h) {
+    if (nscheme == 41 && L.ist > 1 && h <= 5) {
+        if (h == 0) return s1_state(L, m, 0);
+        if (h == 2) return s3_left(L, m, 2);
+        return s2_left(L, m, h);
+    }
+    return qwl_postB(L, sqwl, m, h);
+}
+
+__global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+                                                   const LineGroup *__restrict__ groups, int dir, int nl_max,
+                                                   int hmax, int *err) {
+    extern __shared__ double smem[];
+    const LineGroup G = groups[blockIdx.x];
+    const DevBlock B = blocks[G.blk];
+    const int n = dimof(B, dir);
+    const int H = n + 1;
+    const int NL = G.nl;
+    double *sqwl = smem;                       // NL * 5 * H
+    double *sqwr = sqwl + (size_t)nl_max * 5 * hmax;
+    double *sf = sqwr + (size_t)nl_max * 5 * hmax;
+    double *ssec = sf + (size_t)nl_max * 5 * hmax;  // NL * 26 * 5
+    __shared__ InvLine lines[8];
+    const int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
+    if (threadIdx.x < NL) {
+        int c[3];
+        c[a1] = G.a0 + threadIdx.x;
+        c[a2] = G.b;
+        c[dir] = -2;
+        long long base = gidx(B, c[0], c[1], c[2]);
+        InvLine L;
+        for (int m = 0; m < 5; m++) L.q[m] = F.f[F_R + m] + base;
+        L.stride = dstride(B, dir);
+        L.dqbase = base + 2 * L.stride;
+        L.n = n;
+        L.ist = __ldg(F.f[F_R] + base) < SMALL ? 2 : 0;
+        L.ied = __ldg(F.f[F_R] + base + (long long)(n + 5) * L.stride) < SMALL ? n - 2 : n;
+        lines[threadIdx.x] = L;
+    }
+    __syncthreads();
+    const bool posmajor = (dir == 0);
+    const double CL[3] = {1.0 / 16.0, 10.0 / 16.0, 5.0 / 16.0};
+    const double CR[3] = {5.0 / 16.0, 10.0 / 16.0, 1.0 / 16.0};
+    const double EPS = 1.0e-6;
+
+    // ---- phase A: weights per point i in [ist, ied+1]
+    {
+        const int NP = n + 2;  // i in 0..n+1
+        for (int idx = threadIdx.x; idx < NL * NP; idx += blockDim.x) {
+            int ln = posmajor ? idx / NP : idx % NL;
+            int i = posmajor ? idx % NP : idx / NL;
+            const InvLine &L = lines[ln];
+            if (i < L.ist || i > L.ied + 1) continue;
+            double *ql_ = sqwl + (size_t)ln * 5 * H;
+            double *qr_ = sqwr + (size_t)ln * 5 * H;
+            for (int m = 0; m < 5; m++) {
+                double qm2 = qv(L, m, i - 2), qm1 = qv(L, m, i - 1), q0 = qv(L, m, i), qp1 = qv(L, m, i + 1),
+                       qp2 = qv(L, m, i + 2);
+                double g[3], s[3], bl[3], br[3];
+                g[0] = 0.5 * (qm2 - 4.0 * qm1 + 3.0 * q0);
+                g[1] = 0.5 * (qp1 - qm1);
+                g[2] = 0.5 * (-3.0 * q0 + 4.0 * qp1 - qp2);
+                s[0] = qm2 - 2.0 * qm1 + q0;
+                s[1] = qm1 - 2.0 * q0 + qp1;
+                s[2] = q0 - 2.0 * qp1 + qp2;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    double IS = g[k] * g[k] + s[k] * s[k];
+                    double t = EPS + IS;
+                    double EIS2 = t * t;
+                    bl[k] = CL[k] / EIS2;
+                    br[k] = CR[k] / EIS2;
+                }
+                if (i <= L.ied) {
+                    double IS = bl[0] + bl[1] + bl[2];
+                    double w0 = bl[0] / IS, w1 = bl[1] / IS, w2 = bl[2] / IS;
+                    ql_[m * H + i] = q0 + 0.125 * (w0 * (s[0] + 4.0 * g[0]) + w1 * (s[1] + 4.0 * g[1]) + w2 * (s[2] + 4.0 * g[2]));
+                }
+                if (i - 1 >= L.ist) {
+                    double IS = br[0] + br[1] + br[2];
+                    double w0 = br[0] / IS, w1 = br[1] / IS, w2 = br[2] / IS;
+                    qr_[m * H + i - 1] = q0 + 0.125 * (w0 * (s[0] - 4.0 * g[0]) + w1 * (s[1] - 4.0 * g[1]) + w2 * (s[2] - 4.0 * g[2]));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // ---- phase B: fluxes at half nodes, and boundary-section fluxes
+    {
+        const int NT = H + 26;
+        int nbad = 0;
+        for (int idx = threadIdx.x; idx < NL * NT; idx += blockDim.x) {
+            int ln = posmajor ? idx / NT : idx % NL;
+            int t = posmajor ? idx % NT : idx / NL;
+            const InvLine &L = lines[ln];
+            const double *ql_ = sqwl + (size_t)ln * 5 * H;
+            const double *qr_ = sqwr + (size_t)ln * 5 * H;
+            double ql[5], qr[5], fl[5];
+            int h, mode = 0;  // 0 main, 1..6 sections
+            if (t < H) {
+                h = t;
+                for (int m = 0; m < 5; m++) { ql[m] = qwl_postB(L, ql_, m, h); qr[m] = qwr_postB(L, qr_, m, h); }
+                if (ql[0] <= RMIN_LIMIT || ql[4] <= PMIN_LIMIT) { int ii = h > 1 ? h : 1; for (int m = 0; m < 5; m++) ql[m] = qv(L, m, ii); }
+                if (qr[0] <= RMIN_LIMIT || qr[4] <= PMIN_LIMIT) { int ii = h + 1 < n ? h + 1 : n; for (int m = 0; m < 5; m++) qr[m] = qv(L, m, ii); }
+            } else {
+                if (P.nscheme != 41) continue;
+                int s = t - H;  // 0..25
+                if (s < 13) {
+                    if (L.ist <= 1) continue;
+                    if (s < 4) { mode = 1; h = s; }
+                    else if (s < 9) { mode = 2; h = s - 4 + 1; }
+                    else { mode = 3; h = s - 9 + 1; }
+                } else {
+                    if (L.ied >= n) continue;
+                    int r = s - 13;
+                    if (r < 4) { mode = 4; h = n - r; }
+                    else if (r < 9) { mode = 5; h = n - 1 - (r - 4); }
+                    else { mode = 6; h = n - 1 - (r - 9); }
+                }
+                for (int m = 0; m < 5; m++) {
+                    switch (mode) {
+                    case 1: ql[m] = qr[m] = s1_state(L, m, h); break;
+                    case 2: ql[m] = s2_left(L, m, h); qr[m] = s2_right(L, m, h); break;
+                    case 3: ql[m] = s3_left(L, m, h); qr[m] = qwr_postB(L, qr_, m, h); break;
+                    case 4: ql[m] = qr[m] = s4_state(L, m, h); break;
+                    case 5: ql[m] = s5_left(L, m, h); qr[m] = s5_right(L, m, h); break;
+                    default: ql[m] = qwl_preright(L, ql_, P.nscheme, m, h); qr[m] = s6_right(L, m, h); break;
+                    }
+                }
+                bool badl = ql[0] <= RMIN_LIMIT || ql[4] <= PMIN_LIMIT;
+                bool badr = qr[0] <= RMIN_LIMIT || qr[4] <= PMIN_LIMIT;
+                int ia = h > 1 ? h : 1, ib = h + 1 < n ? h + 1 : n;
+                for (int m = 0; m < 5; m++) {
+                    if (mode == 1) {
+                        if (badl) ql[m] = (qv(L, m, ia) + qv(L, m, h + 1)) / 2.;
+                        if (badr) qr[m] = (qv(L, m, ia) + qv(L, m, h + 1)) / 2.;
+                    } else if (mode == 4) {
+                        if (badl) ql[m] = (qv(L, m, 1) + qv(L, m, h)) / 2.0;
+                        if (badr) qr[m] = (qv(L, m, 1) + qv(L, m, h)) / 2.0;
+                    } else {
+                        if (badl) ql[m] = qv(L, m, ia);
+                        if (badr) qr[m] = qv(L, m, ib);
+                    }
+                }
+            }
+            // half-node metrics: VALUE_HALF_NODE of (kx,ky,kz) along the line
+            const double *mx = F.f[F_KCX + 3 * dir] + L.dqbase, *my = F.f[F_KCX + 3 * dir + 1] + L.dqbase,
+                         *mz = F.f[F_KCX + 3 * dir + 2] + L.dqbase;
+            long long st = L.stride;
+            auto ax = [&](int l) { return __ldg(mx + (long long)l * st); };
+            auto ay = [&](int l) { return __ldg(my + (long long)l * st); };
+            auto az = [&](int l) { return __ldg(mz + (long long)l * st); };
+            double kx = value_half_node_at(ax, n, h), ky = value_half_node_at(ay, n, h), kz = value_half_node_at(az, n, h);
+            const double kt = 0.0;  // kct=0, so every half-node value of kt is +0
+            nbad += flux_type(P, ql, qr, kx, ky, kz, kt, fl);
+            if (mode == 0) {
+                double *f_ = sf + (size_t)ln * 5 * H;
+                for (int m = 0; m < 5; m++) f_[m * H + h] = fl[m];
+            } else {
+                double *sc = ssec + (size_t)ln * 26 * 5 + (size_t)(t - H) * 5;
+                for (int m = 0; m < 5; m++) sc[m] = fl[m];
+            }
+        }
+        if (nbad) atomicAdd(&err[ERR_ROE], nbad);
+    }
+    __syncthreads();
+    // ---- phase C: flux difference and accumulation into dq
+    {
+        for (int idx = threadIdx.x; idx < NL * n; idx += blockDim.x) {
+            int ln = posmajor ? idx / n : idx % NL;
+            int l = 1 + (posmajor ? idx % n : idx / NL);
+            const InvLine &L = lines[ln];
+            const double *f_ = sf + (size_t)ln * 5 * H;
+            const double *sc = ssec + (size_t)ln * 26 * 5;
+            bool right = P.nscheme == 41 && L.ied < n && l >= n - 2;
+            bool left = P.nscheme == 41 && L.ist > 1 && l <= 3;
+            long long gi = L.dqbase + (long long)l * L.stride;
+            for (int m = 0; m < 5; m++) {
+                double df;
+                if (right) {
+                    const double *s4 = sc + 13 * 5, *s5 = sc + 17 * 5, *s6 = sc + 22 * 5;
+                    // section fluxes f(ni-h): s4[k] holds f(k), s5[k] holds f(k+1), s6[k] holds f(k+1)
+                    if (l == n) df = -(-23.0 * s4[0 * 5 + m] + 21.0 * s4[1 * 5 + m] + 3.0 * s4[2 * 5 + m] - 1.0 * s4[3 * 5 + m]) / 24.0;
+                    else if (l == n - 1) df = -(-22.0 * s5[0 * 5 + m] + 17.0 * s5[1 * 5 + m] + 9.0 * s5[2 * 5 + m] - 5.0 * s5[3 * 5 + m] + s5[4 * 5 + m]) / 24.0;
+                    else df = -(s6[0 * 5 + m] - 27.0 * s6[1 * 5 + m] + 27.0 * s6[2 * 5 + m] - s6[3 * 5 + m]) / 24.0;
+                } else if (left) {
+                    const double *s1 = sc, *s2 = sc + 4 * 5, *s3 = sc + 9 * 5;
+                    if (l == 1) df = (-23.0 * s1[0 * 5 + m] + 21.0 * s1[1 * 5 + m] + 3.0 * s1[2 * 5 + m] - 1.0 * s1[3 * 5 + m]) / 24.0;
+                    else if (l == 2) df = (-22.0 * s2[0 * 5 + m] + 17.0 * s2[1 * 5 + m] + 9.0 * s2[2 * 5 + m] - 5.0 * s2[3 * 5 + m] + s2[4 * 5 + m]) / 24.0;
+                    else df = (s3[0 * 5 + m] - 27.0 * s3[1 * 5 + m] + 27.0 * s3[2 * 5 + m] - s3[3 * 5 + m]) / 24.0;
+                } else {
+                    auto fa = [&](int hh) { return f_[m * H + hh]; };
+                    df = flux_dxyz_at(fa, n, l);
+                }
+                double *dq = F.f[F_DQ1 + m];
+                dq[gi] = dq[gi] + df;
+            }
+        }
+    }
+}
+
+void launch_rhs_invis(const LaunchCtx &c, int dir) {
+    const DirTable &T = c.inv[dir];
+    if (T.ngroups == 0) return;
+    size_t smem = (size_t)T.nl_max * (15 * (size_t)T.hmax + 26 * 5) * sizeof(double);
+    k_rhs_invis<<<T.ngroups, 256, smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, T.nl_max, T.hmax, c.err);
+}
+
+void setup_rhs_invis_attrs(size_t max_smem) {
+    cudaFuncSetAttribute(k_rhs_invis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+}
+
+}  // namespace wcns

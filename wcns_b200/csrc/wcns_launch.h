@@ -1,0 +1,95 @@
+// wcns_launch.h -- host-side launch context shared by the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+#include "wcns_dev.cuh"
+
+namespace wcns {
+
+// A group of up to 8 lines of one block along direction `dir`: lines are
+// indexed by (a, b) = the two other indices, a running fastest in memory for
+// dir != 0 (so that a group reads coalesced rows) and along j for dir == 0.
+struct LineGroup {
+    int blk, a0, b, nl;
+};
+
+struct DirTable {
+    LineGroup *groups = nullptr;  // device
+    int ngroups = 0, nl_max = 0, hmax = 0;
+};
+
+// One boundary region as the device sees it (bcindex order within a block).
+struct DevRegion {
+    int blk, bctype;
+    int s_st[3], s_ed[3];
+    int s_nd, s_lr, s_lr3d[3];
+};
+
+// interface ghost copy: ghost (dst) <- partner interior (src)
+struct GhostCopy {
+    long long dst, src;
+};
+
+// interface averaging entry: own face point <- partner face point
+struct PairEntry {
+    long long own, partner;  // field indices
+    int partner_slot;        // index of the partner point in the snapshot list
+    int same;                // 1 for a block connected to itself
+};
+
+struct LaunchCtx {
+    cudaStream_t stream = 0;
+    const DevParams *P = nullptr;  // host copy, passed by value
+    const DevFields *F = nullptr;
+    DevBlock *blocks = nullptr;    // device
+    const DevBlock *hblocks = nullptr;
+    int nblocks = 0;
+    int *err = nullptr;            // device error slots
+    DirTable inv[3], vis[3];
+    // boundary conditions
+    GhostCopy *ghost = nullptr;
+    long long nghost = 0;
+    DevRegion *regions = nullptr;  // physical regions, grouped per block in bcindex order
+    int *reg_first = nullptr;      // per block: first region index (nblocks+1 entries), device
+    int max_regions_per_block = 0;
+    // dq-zero list (points on physical faces)
+    long long *zero_pts = nullptr;
+    long long nzero = 0;
+    // interface averaging
+    long long *snap_pts = nullptr;  // field index of every interface face point
+    int nsnap = 0;
+    double *snap = nullptr;         // 6 * nsnap
+    PairEntry *pairs = nullptr;     // grouped per block, region order
+    int *pair_first = nullptr;      // per block (nblocks+1), device
+    int *reg_pair_first = nullptr;  // per block per region boundaries (flattened), device
+    int *blk_reg_first = nullptr;   // per block index into reg_pair_first, device
+    int max_pair_regions = 0;
+    int ncomp = 0, nmem = 0;
+    int *comp_first = nullptr, *comp_n = nullptr, *mem_slot = nullptr;
+    int *mem_comp = nullptr;
+    long long *mem_idx = nullptr;
+    // residual
+    double *res_partial = nullptr;  // per CTA partial sums
+    int res_ctas_per_block = 0;
+    double *res_out = nullptr;      // per block: res, resmax; then rms
+    // update bad-point lists
+    int *bad_count = nullptr;       // per block
+    long long *bad_list = nullptr;  // per block, capacity BAD_CAP
+};
+
+constexpr int BAD_CAP = 512;
+
+void launch_rhs_invis(const LaunchCtx &c, int dir);
+void setup_rhs_invis_attrs(size_t max_smem);
+void launch_node_derivatives(const LaunchCtx &c);
+void launch_rhs_vis(const LaunchCtx &c, int dir);
+void setup_rhs_vis_attrs(size_t max_smem);
+void launch_boundary(const LaunchCtx &c);
+void launch_init(const LaunchCtx &c);
+void launch_timestep(const LaunchCtx &c);
+void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
+void launch_lhs(const LaunchCtx &c);
+void launch_update(const LaunchCtx &c);
+void launch_residual(const LaunchCtx &c, double *rms_slot);
+void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
+
+}  // namespace wcns

@@ -1,0 +1,144 @@
+"""Host-side mirror of the reference's per-step interface for the WCNS path.
+
+The reference drives its hot path from the Fortran time loop
+(``Main.f90:79-127``) through argument-less subroutines acting on module
+globals.  :class:`Wcns` keeps the same phase names and order, each one a call
+into the C ABI of ``libwcns_b200.so`` (``include/wcns_b200.h``).  Errors the
+reference answers with ``stop`` (Roe ``c^2 <= 0``, too many non-physical
+points, unknown BC type) raise :class:`WcnsError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+FIELDS = ["r", "u", "v", "w", "p", "t", "dq1", "dq2", "dq3", "dq4", "dq5", "dtdt", "sra", "srb", "src",
+          "srva", "srvb", "srvc", "kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz", "vol"]
+FID = {n: i for i, n in enumerate(FIELDS)}
+
+
+class WcnsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _check(rc):
+    if rc != 0:
+        raise WcnsError(rc, _lib.last_error())
+
+
+def params_struct(p) -> _lib.WcnsParams:
+    return _lib.WcnsParams(p.moo, p.attack, p.sideslip, p.reynolds, p.tref, p.twall, p.cfl, p.timedt_rate, p.efix,
+                           p.csrv, p.nvis, p.nscheme, p.nflux, 0)
+
+
+class Wcns:
+    """One multi-block case resident on the GPU."""
+
+    def __init__(self, case):
+        L = _lib.load()
+        self.case = case
+        self.dims = [tuple(int(v) for v in d) for d in case.dims]
+        self._prm = params_struct(case.params)
+        dims = (C.c_int * (3 * len(self.dims)))(*[v for d in self.dims for v in d])
+        keep, ptrs = [], []
+        for xyz in case.xyz:
+            for a in xyz:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                keep.append(a)
+                ptrs.append(a.ctypes.data)
+        xyz_p = (C.c_void_p * len(ptrs))(*ptrs)
+        regs = np.ascontiguousarray(case.regions, dtype=np.int32)
+        h = C.c_void_p()
+        _check(L.wcns_create(C.byref(self._prm), len(self.dims), dims, xyz_p, regs.shape[0],
+                             regs.ctypes.data_as(C.POINTER(C.c_int)), C.byref(h)))
+        self.h = h
+        for nb, prim in enumerate(case.prim, start=1):
+            self.set_prim(nb, prim)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().wcns_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state -------------------------------------------------------------
+    def set_prim(self, nb, prim):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in prim]
+        _check(_lib.load().wcns_set_prim(self.h, nb, *[a.ctypes.data for a in arrs]))
+
+    def get(self, name, nb, out=None):
+        """Copy one field of block nb (ghosted layout) to host memory."""
+        ni, nj, nk = self.dims[nb - 1]
+        if out is None:
+            out = np.empty((nk + 6, nj + 6, ni + 6))
+        elif out.shape != (nk + 6, nj + 6, ni + 6) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("output array has the wrong shape, dtype or layout")
+        _check(_lib.load().wcns_get_field(self.h, FID[name], nb, out.ctypes.data))
+        return out
+
+    def set(self, name, nb, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        _check(_lib.load().wcns_set_field(self.h, FID[name], nb, arr.ctypes.data))
+
+    # -- per-step phases, reference names (Main.f90:85-109) -----------------
+    def boundary_all(self):
+        _check(_lib.load().wcns_boundary_all(self.h))
+
+    def initial_q_dq_c_t(self):
+        _check(_lib.load().wcns_initial_q_dq_c_t(self.h))
+
+    def timestep_tgh(self):
+        _check(_lib.load().wcns_timestep(self.h))
+
+    def r_h_s_vis(self):
+        _check(_lib.load().wcns_rhs_vis(self.h))
+
+    def communicate_dq_npp(self):
+        _check(_lib.load().wcns_communicate_dq(self.h))
+
+    def r_h_s_invis(self):
+        _check(_lib.load().wcns_rhs_invis(self.h))
+
+    def l_h_s_tgh(self):
+        _check(_lib.load().wcns_lhs(self.h))
+
+    def communicate_pv_npp(self):
+        _check(_lib.load().wcns_communicate_pv(self.h))
+
+    def residual_curve(self):
+        nb = len(self.dims)
+        res, rmax, rms = np.zeros(nb), np.zeros(nb), np.zeros(1)
+        _check(_lib.load().wcns_residual(self.h, res.ctypes.data, rmax.ctypes.data, rms.ctypes.data))
+        return res, rmax, float(rms[0])
+
+    def step(self, nsteps=1, history=True):
+        """nsteps whole time steps (Main.f90:79-127) replayed from a CUDA graph."""
+        hist = np.zeros(nsteps) if history else None
+        _check(_lib.load().wcns_step(self.h, nsteps, hist.ctypes.data if history else None))
+        return hist
+
+    def step_async(self, nsteps):
+        _check(_lib.load().wcns_step_async(self.h, nsteps))
+
+    def sync(self):
+        _check(_lib.load().wcns_sync(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(_lib.load().wcns_stream(self.h) or 0)
+
+    def launches_per_step(self) -> int:
+        return int(_lib.load().wcns_launches_per_step(self.h))
+
+    def n_multipoints(self) -> int:
+        return int(_lib.load().wcns_n_multipoints(self.h))
