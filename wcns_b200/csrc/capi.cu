@@ -14,6 +14,7 @@
 // block connected to itself uses the in-place same-rank path.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -78,7 +79,10 @@ struct WcnsContext {
     DevFields F{};
     std::vector<HBlock> blk;  // 0-based
     long long total = 0;      // ghosted points over all blocks
+    long long total_pm = 0;   // plane-major sweep points over all blocks
     double *pool = nullptr;
+    double *pm_pool = nullptr;
+    PmFields PM{};
     cudaStream_t stream = nullptr;
     LaunchCtx L;
     std::vector<void *> owned;  // device allocations to free
@@ -92,6 +96,7 @@ struct WcnsContext {
         if (graph) cudaGraphExecDestroy(graph);
         for (void *p : owned) cudaFree(p);
         if (pool) cudaFree(pool);
+        if (pm_pool) cudaFree(pm_pool);
         if (stream) cudaStreamDestroy(stream);
     }
     template <class T>
@@ -384,18 +389,21 @@ static int build_tables(WcnsContext *c) {
         for (int pass = 0; pass < 2; pass++) {  // 0 inviscid, 1 viscous
             std::vector<LineGroup> g;
             int nl_max = 0, hmax = 0;
+            size_t sm_dir = 0;
             for (int b = 0; b < nbk; b++) {
                 const DevBlock &D = c->blk[b].d;
                 int n = dimof(D, dir);
                 if (pass == 0 && n <= NIJK2D) continue;
                 int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
                 int na = dimof(D, a1), nb2 = dimof(D, a2);
-                int NL = std::max(1, std::min(8, 512 / (n + 1)));
+                int NL = pass == 0 ? std::max(1, std::min(8, 1536 / (5 * (n + 2)))) : std::max(1, std::min(8, 512 / (n + 1)));
+                size_t per_line = pass == 0 ? (15 * (size_t)(n + 1) + 130) * 8 : 5 * (size_t)(n + 1) * 8;
                 for (int bb = 1; bb <= nb2; bb++)
                     for (int a = 1; a <= na; a += NL) {
                         LineGroup lg{b, a, bb, std::min(NL, na - a + 1)};
                         g.push_back(lg);
                         nl_max = std::max(nl_max, lg.nl);
+                        sm_dir = std::max(sm_dir, per_line * lg.nl);
                     }
                 hmax = std::max(hmax, n + 1);
             }
@@ -403,8 +411,9 @@ static int build_tables(WcnsContext *c) {
             T.ngroups = (int)g.size();
             T.nl_max = nl_max;
             T.hmax = hmax;
+            T.smem = sm_dir;
             T.groups = c->up(g);
-            size_t sm = pass == 0 ? (size_t)nl_max * (15 * (size_t)hmax + 130) * 8 : (size_t)nl_max * 5 * (size_t)hmax * 8;
+            size_t sm = sm_dir;
             if (pass == 0) inv_smem = std::max(inv_smem, sm);
             else vis_smem = std::max(vis_smem, sm);
         }
@@ -412,6 +421,12 @@ static int build_tables(WcnsContext *c) {
     if (inv_smem > 227 * 1024 || vis_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
     setup_rhs_invis_attrs(std::max<size_t>(inv_smem, 48 * 1024));
     setup_rhs_vis_attrs(std::max<size_t>(vis_smem, 48 * 1024));
+    // LU-SGS cluster shape (CTAs per block); WCNS_SWEEP_CLUSTER overrides for tuning
+    {
+        int cl = 16;
+        if (const char *e = getenv("WCNS_SWEEP_CLUSTER")) cl = atoi(e);
+        if (setup_sweep(L, cl)) { set_err("a block has too many (j,k) columns for the sweep kernel"); return WCNS_ERR_ARGUMENT; }
+    }
     // residual partials, update bad lists
     L.res_ctas_per_block = 32;
     CK(cudaMalloc(&L.res_partial, sizeof(double) * 2 * 32 * nbk));
@@ -433,6 +448,7 @@ static int check_errors(WcnsContext *c) {
     CK(cudaMemset(c->d_err, 0, sizeof h));
     if (h[ERR_ROE]) { set_err("flux_Roe: c^2 <= 0 at " + std::to_string(h[ERR_ROE]) + " half nodes"); return WCNS_ERR_ROE; }
     if (h[ERR_UPDATE_BLOCKS]) { set_err("update_limited: too many non-physical points"); return WCNS_ERR_UPDATE; }
+    if (h[ERR_TIMEOUT]) { set_err("LU-SGS sweep: a bounded wait for a plane's coefficients ran out"); return WCNS_ERR_CUDA; }
     return 0;
 }
 
@@ -495,6 +511,9 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
         d.gz = d.nk + 6;
         d.off = off;
         d.npts = (long long)d.ni * d.nj * d.nk;
+        d.pmoff = c->total_pm;
+        c->total_pm += (long long)(d.ni + d.nj + d.nk - 2) * d.nj * d.nk;
+        c->total_pm = (c->total_pm + 31) / 32 * 32;
         off += (long long)d.gx * d.gy * d.gz;
         off = (off + 31) / 32 * 32;
     }
@@ -526,24 +545,35 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     if (cudaMalloc(&c->pool, bytes) != cudaSuccess) { delete c; set_err("device allocation of the field pool failed"); return WCNS_ERR_CUDA; }
     cudaMemset(c->pool, 0, bytes);
     for (int f = 0; f < F_NALL; f++) c->F.f[f] = c->pool + (size_t)f * c->total;
+    // sweep arrays, plane-major: dq (5 planes of values), the static records
+    // (SR_N per cell) and the dynamic records (DYN_N per cell)
+    size_t pmbytes = sizeof(double) * (size_t)(5 + SR_N + DYN_N) * (size_t)c->total_pm;
+    if (cudaMalloc(&c->pm_pool, pmbytes) != cudaSuccess) { delete c; set_err("device allocation of the sweep arrays failed"); return WCNS_ERR_CUDA; }
+    cudaMemset(c->pm_pool, 0, pmbytes);
+    for (int m = 0; m < 5; m++) c->PM.dq[m] = c->pm_pool + (size_t)m * c->total_pm;
+    c->PM.stat = c->pm_pool + (size_t)5 * c->total_pm;
+    c->PM.dyn = c->PM.stat + (size_t)SR_N * c->total_pm;
     std::vector<DevBlock> hb(nblocks);
     for (int b = 0; b < nblocks; b++) hb[b] = c->blk[b].d;
     LaunchCtx &L = c->L;
     L.stream = c->stream;
     L.P = &c->P;
     L.F = &c->F;
+    L.PM = &c->PM;
     L.nblocks = nblocks;
     L.blocks = c->up(hb);
+    {
+        auto *hbl = new DevBlock[nblocks];
+        for (int b = 0; b < nblocks; b++) hbl[b] = hb[b];
+        L.hblocks = hbl;
+    }
     rc = build_tables(c);
     if (rc) { delete c; return rc; }
+    c->PM.csize = L.sweep_cluster;
     CK(cudaMalloc(&c->d_err, sizeof(int) * ERR_NSLOTS));
     c->owned.push_back(c->d_err);
     CK(cudaMemset(c->d_err, 0, sizeof(int) * ERR_NSLOTS));
     L.err = c->d_err;
-    // host block table the launchers read
-    auto *hbl = new DevBlock[nblocks];
-    for (int b = 0; b < nblocks; b++) hbl[b] = hb[b];
-    L.hblocks = hbl;
     // grid metrics on the device
     double *xyzd = nullptr, *work = nullptr;
     CK(cudaMalloc(&xyzd, sizeof(double) * 3 * (size_t)c->total));
@@ -671,7 +701,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     }
     for (int d = 0; d < 3; d++) { launch_rhs_invis(L, d); n += L.inv[d].ngroups ? 1 : 0; }
     launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
-    launch_lhs(L); n += 4 + (L.nzero ? 2 : 0);
+    launch_lhs(L); n += 8 + (L.nzero ? 2 : 0);
     launch_update(L); n += 2;
     launch_communicate(L, 1); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
     launch_residual(L, rms_slot); n += 2;

@@ -126,18 +126,14 @@ __device__ __forceinline__ double qwl_preright(const InvLine &L, const double *s
 }
 
 __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
-                                                   const LineGroup *__restrict__ groups, int dir, int nl_max,
-                                                   int hmax, int *err) {
+                                                   const LineGroup *__restrict__ groups, int dir, int *err) {
     extern __shared__ double smem[];
     const LineGroup G = groups[blockIdx.x];
     const DevBlock B = blocks[G.blk];
     const int n = dimof(B, dir);
     const int H = n + 1;
     const int NL = G.nl;
-    double *sqwl = smem;                       // NL * 5 * H
-    double *sqwr = sqwl + (size_t)nl_max * 5 * hmax;
-    double *sf = sqwr + (size_t)nl_max * 5 * hmax;
-    double *ssec = sf + (size_t)nl_max * 5 * hmax;  // NL * 26 * 5
+    const size_t per_line = (size_t)15 * H + 130;  // qwl, qwr, f (5 x H each) and 26 section fluxes
     __shared__ InvLine lines[8];
     const int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
     if (threadIdx.x < NL) {
@@ -161,49 +157,48 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
     const double CR[3] = {5.0 / 16.0, 10.0 / 16.0, 1.0 / 16.0};
     const double EPS = 1.0e-6;
 
-    // ---- phase A: weights per point i in [ist, ied+1]
+    // ---- phase A: weights per (line, variable, point i in [ist, ied+1])
     {
-        const int NP = n + 2;  // i in 0..n+1
-        for (int idx = threadIdx.x; idx < NL * NP; idx += blockDim.x) {
-            int ln = posmajor ? idx / NP : idx % NL;
-            int i = posmajor ? idx % NP : idx / NL;
+        const int NP = n + 2;
+        const int nitems = NL * 5 * NP;
+        for (int idx = threadIdx.x; idx < nitems; idx += blockDim.x) {
+            int ln, m, i;
+            if (posmajor) { i = idx % NP; m = (idx / NP) % 5; ln = idx / (5 * NP); }
+            else { ln = idx % NL; m = (idx / NL) % 5; i = idx / (5 * NL); }
             const InvLine &L = lines[ln];
             if (i < L.ist || i > L.ied + 1) continue;
-            double *ql_ = sqwl + (size_t)ln * 5 * H;
-            double *qr_ = sqwr + (size_t)ln * 5 * H;
-            for (int m = 0; m < 5; m++) {
-                double qm2 = qv(L, m, i - 2), qm1 = qv(L, m, i - 1), q0 = qv(L, m, i), qp1 = qv(L, m, i + 1),
-                       qp2 = qv(L, m, i + 2);
-                double g[3], s[3], bl[3], br[3];
-                g[0] = 0.5 * (qm2 - 4.0 * qm1 + 3.0 * q0);
-                g[1] = 0.5 * (qp1 - qm1);
-                g[2] = 0.5 * (-3.0 * q0 + 4.0 * qp1 - qp2);
-                s[0] = qm2 - 2.0 * qm1 + q0;
-                s[1] = qm1 - 2.0 * q0 + qp1;
-                s[2] = q0 - 2.0 * qp1 + qp2;
+            double *ql_ = smem + (size_t)ln * per_line;
+            double *qr_ = ql_ + (size_t)5 * H;
+            double qm2 = qv(L, m, i - 2), qm1 = qv(L, m, i - 1), q0 = qv(L, m, i), qp1 = qv(L, m, i + 1), qp2 = qv(L, m, i + 2);
+            double g[3], sdv[3], bl[3], br[3];
+            g[0] = 0.5 * (qm2 - 4.0 * qm1 + 3.0 * q0);
+            g[1] = 0.5 * (qp1 - qm1);
+            g[2] = 0.5 * (-3.0 * q0 + 4.0 * qp1 - qp2);
+            sdv[0] = qm2 - 2.0 * qm1 + q0;
+            sdv[1] = qm1 - 2.0 * q0 + qp1;
+            sdv[2] = q0 - 2.0 * qp1 + qp2;
 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    double IS = g[k] * g[k] + s[k] * s[k];
-                    double t = EPS + IS;
-                    double EIS2 = t * t;
-                    bl[k] = CL[k] / EIS2;
-                    br[k] = CR[k] / EIS2;
-                }
-                if (i <= L.ied) {
-                    double IS = bl[0] + bl[1] + bl[2];
-                    double w0 = bl[0] / IS, w1 = bl[1] / IS, w2 = bl[2] / IS;
-                    ql_[m * H + i] = q0 + 0.125 * (w0 * (s[0] + 4.0 * g[0]) + w1 * (s[1] + 4.0 * g[1]) + w2 * (s[2] + 4.0 * g[2]));
-                }
-                if (i - 1 >= L.ist) {
-                    double IS = br[0] + br[1] + br[2];
-                    double w0 = br[0] / IS, w1 = br[1] / IS, w2 = br[2] / IS;
-                    qr_[m * H + i - 1] = q0 + 0.125 * (w0 * (s[0] - 4.0 * g[0]) + w1 * (s[1] - 4.0 * g[1]) + w2 * (s[2] - 4.0 * g[2]));
-                }
+            for (int kk = 0; kk < 3; kk++) {
+                double IS = g[kk] * g[kk] + sdv[kk] * sdv[kk];
+                double tt = EPS + IS;
+                double EIS2 = tt * tt;
+                bl[kk] = CL[kk] / EIS2;
+                br[kk] = CR[kk] / EIS2;
+            }
+            if (i <= L.ied) {
+                double IS = bl[0] + bl[1] + bl[2];
+                double w0 = bl[0] / IS, w1 = bl[1] / IS, w2 = bl[2] / IS;
+                ql_[m * H + i] = q0 + 0.125 * (w0 * (sdv[0] + 4.0 * g[0]) + w1 * (sdv[1] + 4.0 * g[1]) + w2 * (sdv[2] + 4.0 * g[2]));
+            }
+            if (i - 1 >= L.ist) {
+                double IS = br[0] + br[1] + br[2];
+                double w0 = br[0] / IS, w1 = br[1] / IS, w2 = br[2] / IS;
+                qr_[m * H + i - 1] = q0 + 0.125 * (w0 * (sdv[0] - 4.0 * g[0]) + w1 * (sdv[1] - 4.0 * g[1]) + w2 * (sdv[2] - 4.0 * g[2]));
             }
         }
     }
     __syncthreads();
-    // ---- phase B: fluxes at half nodes, and boundary-section fluxes
+    // ---- phase B: fluxes at half nodes, and the nscheme=41 boundary-section fluxes
     {
         const int NT = H + 26;
         int nbad = 0;
@@ -211,8 +206,8 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
             int ln = posmajor ? idx / NT : idx % NL;
             int t = posmajor ? idx % NT : idx / NL;
             const InvLine &L = lines[ln];
-            const double *ql_ = sqwl + (size_t)ln * 5 * H;
-            const double *qr_ = sqwr + (size_t)ln * 5 * H;
+            const double *ql_ = smem + (size_t)ln * per_line;
+            const double *qr_ = ql_ + (size_t)5 * H;
             double ql[5], qr[5], fl[5];
             int h, mode = 0;  // 0 main, 1..6 sections
             if (t < H) {
@@ -222,15 +217,15 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
                 if (qr[0] <= RMIN_LIMIT || qr[4] <= PMIN_LIMIT) { int ii = h + 1 < n ? h + 1 : n; for (int m = 0; m < 5; m++) qr[m] = qv(L, m, ii); }
             } else {
                 if (P.nscheme != 41) continue;
-                int s = t - H;  // 0..25
-                if (s < 13) {
+                int sidx = t - H;  // 0..25
+                if (sidx < 13) {
                     if (L.ist <= 1) continue;
-                    if (s < 4) { mode = 1; h = s; }
-                    else if (s < 9) { mode = 2; h = s - 4 + 1; }
-                    else { mode = 3; h = s - 9 + 1; }
+                    if (sidx < 4) { mode = 1; h = sidx; }
+                    else if (sidx < 9) { mode = 2; h = sidx - 4 + 1; }
+                    else { mode = 3; h = sidx - 9 + 1; }
                 } else {
                     if (L.ied >= n) continue;
-                    int r = s - 13;
+                    int r = sidx - 13;
                     if (r < 4) { mode = 4; h = n - r; }
                     else if (r < 9) { mode = 5; h = n - 1 - (r - 4); }
                     else { mode = 6; h = n - 1 - (r - 9); }
@@ -272,47 +267,47 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
             const double kt = 0.0;  // kct=0, so every half-node value of kt is +0
             nbad += flux_type(P, ql, qr, kx, ky, kz, kt, fl);
             if (mode == 0) {
-                double *f_ = sf + (size_t)ln * 5 * H;
+                double *f_ = smem + (size_t)ln * per_line + (size_t)10 * H;
                 for (int m = 0; m < 5; m++) f_[m * H + h] = fl[m];
             } else {
-                double *sc = ssec + (size_t)ln * 26 * 5 + (size_t)(t - H) * 5;
+                double *sc = smem + (size_t)ln * per_line + (size_t)15 * H + (size_t)(t - H) * 5;
                 for (int m = 0; m < 5; m++) sc[m] = fl[m];
             }
         }
         if (nbad) atomicAdd(&err[ERR_ROE], nbad);
     }
     __syncthreads();
-    // ---- phase C: flux difference and accumulation into dq
+    // ---- phase C: flux difference and accumulation into dq, per (line, point, variable)
     {
-        for (int idx = threadIdx.x; idx < NL * n; idx += blockDim.x) {
-            int ln = posmajor ? idx / n : idx % NL;
-            int l = 1 + (posmajor ? idx % n : idx / NL);
+        const int nitems = NL * n * 5;
+        for (int idx = threadIdx.x; idx < nitems; idx += blockDim.x) {
+            int ln, l, m;
+            if (posmajor) { l = 1 + idx % n; m = (idx / n) % 5; ln = idx / (5 * n); }
+            else { ln = idx % NL; m = (idx / NL) % 5; l = 1 + idx / (5 * NL); }
             const InvLine &L = lines[ln];
-            const double *f_ = sf + (size_t)ln * 5 * H;
-            const double *sc = ssec + (size_t)ln * 26 * 5;
+            const double *f_ = smem + (size_t)ln * per_line + (size_t)10 * H;
+            const double *sc = smem + (size_t)ln * per_line + (size_t)15 * H;
             bool right = P.nscheme == 41 && L.ied < n && l >= n - 2;
             bool left = P.nscheme == 41 && L.ist > 1 && l <= 3;
             long long gi = L.dqbase + (long long)l * L.stride;
-            for (int m = 0; m < 5; m++) {
-                double df;
-                if (right) {
-                    const double *s4 = sc + 13 * 5, *s5 = sc + 17 * 5, *s6 = sc + 22 * 5;
-                    // section fluxes f(ni-h): s4[k] holds f(k), s5[k] holds f(k+1), s6[k] holds f(k+1)
-                    if (l == n) df = -(-23.0 * s4[0 * 5 + m] + 21.0 * s4[1 * 5 + m] + 3.0 * s4[2 * 5 + m] - 1.0 * s4[3 * 5 + m]) / 24.0;
-                    else if (l == n - 1) df = -(-22.0 * s5[0 * 5 + m] + 17.0 * s5[1 * 5 + m] + 9.0 * s5[2 * 5 + m] - 5.0 * s5[3 * 5 + m] + s5[4 * 5 + m]) / 24.0;
-                    else df = -(s6[0 * 5 + m] - 27.0 * s6[1 * 5 + m] + 27.0 * s6[2 * 5 + m] - s6[3 * 5 + m]) / 24.0;
-                } else if (left) {
-                    const double *s1 = sc, *s2 = sc + 4 * 5, *s3 = sc + 9 * 5;
-                    if (l == 1) df = (-23.0 * s1[0 * 5 + m] + 21.0 * s1[1 * 5 + m] + 3.0 * s1[2 * 5 + m] - 1.0 * s1[3 * 5 + m]) / 24.0;
-                    else if (l == 2) df = (-22.0 * s2[0 * 5 + m] + 17.0 * s2[1 * 5 + m] + 9.0 * s2[2 * 5 + m] - 5.0 * s2[3 * 5 + m] + s2[4 * 5 + m]) / 24.0;
-                    else df = (s3[0 * 5 + m] - 27.0 * s3[1 * 5 + m] + 27.0 * s3[2 * 5 + m] - s3[3 * 5 + m]) / 24.0;
-                } else {
-                    auto fa = [&](int hh) { return f_[m * H + hh]; };
-                    df = flux_dxyz_at(fa, n, l);
-                }
-                double *dq = F.f[F_DQ1 + m];
-                dq[gi] = dq[gi] + df;
+            double df;
+            if (right) {
+                const double *s4 = sc + 13 * 5, *s5 = sc + 17 * 5, *s6 = sc + 22 * 5;
+                // section fluxes f(ni-h): s4[k] holds f(k), s5[k] and s6[k] hold f(k+1)
+                if (l == n) df = -(-23.0 * s4[0 * 5 + m] + 21.0 * s4[1 * 5 + m] + 3.0 * s4[2 * 5 + m] - 1.0 * s4[3 * 5 + m]) / 24.0;
+                else if (l == n - 1) df = -(-22.0 * s5[0 * 5 + m] + 17.0 * s5[1 * 5 + m] + 9.0 * s5[2 * 5 + m] - 5.0 * s5[3 * 5 + m] + s5[4 * 5 + m]) / 24.0;
+                else df = -(s6[0 * 5 + m] - 27.0 * s6[1 * 5 + m] + 27.0 * s6[2 * 5 + m] - s6[3 * 5 + m]) / 24.0;
+            } else if (left) {
+                const double *s1 = sc, *s2 = sc + 4 * 5, *s3 = sc + 9 * 5;
+                if (l == 1) df = (-23.0 * s1[0 * 5 + m] + 21.0 * s1[1 * 5 + m] + 3.0 * s1[2 * 5 + m] - 1.0 * s1[3 * 5 + m]) / 24.0;
+                else if (l == 2) df = (-22.0 * s2[0 * 5 + m] + 17.0 * s2[1 * 5 + m] + 9.0 * s2[2 * 5 + m] - 5.0 * s2[3 * 5 + m] + s2[4 * 5 + m]) / 24.0;
+                else df = (s3[0 * 5 + m] - 27.0 * s3[1 * 5 + m] + 27.0 * s3[2 * 5 + m] - s3[3 * 5 + m]) / 24.0;
+            } else {
+                auto fa = [&](int hh) { return f_[m * H + hh]; };
+                df = flux_dxyz_at(fa, n, l);
             }
+            double *dq = F.f[F_DQ1 + m];
+            dq[gi] = dq[gi] + df;
         }
     }
 }
@@ -320,8 +315,7 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
 void launch_rhs_invis(const LaunchCtx &c, int dir) {
     const DirTable &T = c.inv[dir];
     if (T.ngroups == 0) return;
-    size_t smem = (size_t)T.nl_max * (15 * (size_t)T.hmax + 26 * 5) * sizeof(double);
-    k_rhs_invis<<<T.ngroups, 256, smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, T.nl_max, T.hmax, c.err);
+    k_rhs_invis<<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, c.err);
 }
 
 void setup_rhs_invis_attrs(size_t max_smem) {

@@ -229,8 +229,7 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
 void launch_rhs_vis(const LaunchCtx &c, int dir) {
     const DirTable &T = c.vis[dir];
     if (T.ngroups == 0) return;
-    size_t smem = (size_t)T.nl_max * 5 * (size_t)T.hmax * sizeof(double);
-    k_rhs_vis<<<T.ngroups, 256, smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, T.hmax);
+    k_rhs_vis<<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, T.hmax);
 }
 
 void setup_rhs_vis_attrs(size_t max_smem) {

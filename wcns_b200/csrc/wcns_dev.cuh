@@ -56,7 +56,50 @@ struct DevBlock {
     int gx, gy, gz;
     long long off;   // base offset of this block in every field
     long long npts;  // ni*nj*nk
+    long long pmoff; // base offset in the plane-major sweep arrays
 };
+
+// Plane-major layout for the LU-SGS sweeps.  Cell (i,j,k) of a block lives
+// in plane p = i+j+k at column slot c(j,k); the cells of one hyperplane are
+// contiguous.  Columns are grouped in j-chunks, one chunk per CTA of the
+// block's sweep cluster: chunk q covers j-1 in [q*nj/C, (q+1)*nj/C) for all
+// k, and slot = j0(q)*nk + (k-1)*width(q) + (j-1-j0(q)).
+__host__ __device__ inline int chunk_j0(int q, int nj, int C) { return (int)(((long long)q * nj) / C); }
+__host__ __device__ inline int chunk_of(int jj, int nj, int C) {  // jj = j-1
+    int q = (int)(((long long)jj * C) / nj);
+    if (q > C - 1) q = C - 1;
+    while (q > 0 && chunk_j0(q, nj, C) > jj) q--;
+    while (q < C - 1 && chunk_j0(q + 1, nj, C) <= jj) q++;
+    return q;
+}
+__host__ __device__ inline int col_slot(int j, int k, int nj, int nk, int C) {
+    int jj = j - 1, q = chunk_of(jj, nj, C);
+    int j0 = chunk_j0(q, nj, C), w = chunk_j0(q + 1, nj, C) - j0;
+    return j0 * nk + (k - 1) * w + (jj - j0);
+}
+
+// static per-cell record of the sweeps (written once per step by k_lhs_prep)
+enum StatRec : int {
+    SR_COED = 0, SR_RHS = 1,              // coed, rhs(5)
+    SR_JS = 6,                            // um, vm, wm, c2, hm, af
+    SR_JD = 12,                           // per direction d: ct, nx, ny, nz at SR_JD + 4d
+    SR_JP = 24,                           // npn=+1 (lower neighbour): l1, x1, x2 at SR_JP + 3d
+    SR_JM = 33,                           // npn=-1 (upper neighbour): l1, x1, x2 at SR_JM + 3d
+    SR_SRV = 42,                          // srva, srvb, srvc
+    SR_N = 46                             // record length (16-byte multiple)
+};
+constexpr int DYN_N = 16;                 // dynamic per-cell record: dq of the previous sweep or old-side terms
+
+struct PmFields {
+    double *dq[5];   // SoA dq in plane-major order (result of every sweep)
+    double *stat;    // [cell][SR_N]
+    double *dyn;     // [cell][DYN_N]
+    int csize;       // CTAs per block cluster (defines the column slots)
+};
+
+__host__ __device__ inline long long pmidx(const DevBlock &b, int p, int slot) {
+    return b.pmoff + (long long)(p - 3) * ((long long)b.nj * b.nk) + slot;
+}
 
 struct DevFields {
     double *f[F_NALL];
@@ -297,6 +340,6 @@ __device__ __forceinline__ double sutherland(const DevParams &P, double tm) {
 }
 
 // error counters
-enum ErrSlot : int { ERR_ROE = 0, ERR_UPDATE_BLOCKS = 1, ERR_BADLIST_OVERFLOW = 2, ERR_NSLOTS = 4 };
+enum ErrSlot : int { ERR_ROE = 0, ERR_UPDATE_BLOCKS = 1, ERR_BADLIST_OVERFLOW = 2, ERR_TIMEOUT = 3, ERR_NSLOTS = 4 };
 
 }  // namespace wcns

@@ -15,6 +15,7 @@ struct LineGroup {
 struct DirTable {
     LineGroup *groups = nullptr;  // device
     int ngroups = 0, nl_max = 0, hmax = 0;
+    size_t smem = 0;              // dynamic shared memory of the launch (max over groups)
 };
 
 // One boundary region as the device sees it (bcindex order within a block).
@@ -71,6 +72,9 @@ struct LaunchCtx {
     double *res_partial = nullptr;  // per CTA partial sums
     int res_ctas_per_block = 0;
     double *res_out = nullptr;      // per block: res, resmax; then rms
+    // LU-SGS sweeps: CTAs per block cluster, columns per CTA, threads per CTA
+    int sweep_cluster = 1, sweep_cpc = 1, sweep_threads = 32;
+    const PmFields *PM = nullptr;  // plane-major sweep arrays
     // update bad-point lists
     int *bad_count = nullptr;       // per block
     long long *bad_list = nullptr;  // per block, capacity BAD_CAP
@@ -88,6 +92,7 @@ void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);
 void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
 void launch_lhs(const LaunchCtx &c);
+int setup_sweep(LaunchCtx &c, int cluster);
 void launch_update(const LaunchCtx &c);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
