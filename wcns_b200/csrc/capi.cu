@@ -421,11 +421,13 @@ static int build_tables(WcnsContext *c) {
     if (inv_smem > 227 * 1024 || vis_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
     setup_rhs_invis_attrs(std::max<size_t>(inv_smem, 48 * 1024));
     setup_rhs_vis_attrs(std::max<size_t>(vis_smem, 48 * 1024));
-    // LU-SGS cluster shape (CTAs per block); WCNS_SWEEP_CLUSTER overrides for tuning
+    // LU-SGS sweep shape; WCNS_SWEEP_CLUSTER (CTAs per block) and WCNS_SWEEP_FINE (0: three
+    // threads per column) override it for tuning
     {
-        int cl = 16;
+        int cl = 16, fine = 1;
         if (const char *e = getenv("WCNS_SWEEP_CLUSTER")) cl = atoi(e);
-        if (setup_sweep(L, cl)) { set_err("a block has too many (j,k) columns for the sweep kernel"); return WCNS_ERR_ARGUMENT; }
+        if (const char *e = getenv("WCNS_SWEEP_FINE")) fine = atoi(e);
+        if (setup_sweep(L, cl, fine)) { set_err("a block has too many (j,k) columns for the sweep kernel"); return WCNS_ERR_ARGUMENT; }
     }
     // residual partials, update bad lists
     L.res_ctas_per_block = 32;
@@ -551,6 +553,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     if (cudaMalloc(&c->pm_pool, pmbytes) != cudaSuccess) { delete c; set_err("device allocation of the sweep arrays failed"); return WCNS_ERR_CUDA; }
     cudaMemset(c->pm_pool, 0, pmbytes);
     for (int m = 0; m < 5; m++) c->PM.dq[m] = c->pm_pool + (size_t)m * c->total_pm;
+    c->PM.dq_stride = c->total_pm;
     c->PM.stat = c->pm_pool + (size_t)5 * c->total_pm;
     c->PM.dyn = c->PM.stat + (size_t)SR_N * c->total_pm;
     std::vector<DevBlock> hb(nblocks);

@@ -20,16 +20,15 @@
 //                that holds the previous sweep's values.
 //   k_sweep      one thread-block cluster per grid block (the reference's
 //                LU-SGS is block-Jacobi, so blocks are independent).  CTA q
-//                of the cluster owns a j-chunk of the block's (j,k) columns,
-//                a thread owns one column and meets its cell once per plane.
-//                The records of a CTA's cells of one plane are contiguous, so
-//                one bulk copy (three planes ahead, mbarrier completion)
-//                stages them.  After computing its new dq a cell pushes its
-//                contributions A*dq to the next plane: the own (i) column
-//                keeps it in registers, the j and k successors receive it in
-//                their CTA's shared-memory inbox (a distributed-shared-memory
-//                store when the successor is in another CTA).  One cluster
-//                barrier per plane orders producers and consumers.
+//                of the cluster owns a j-chunk of the block's (j,k) columns;
+//                a column's lanes meet its cell once per plane.  The records
+//                of a CTA's cells of one plane are contiguous, so one bulk
+//                copy (issued planes ahead, mbarrier completion) stages them.
+//                After computing its new dq a cell pushes its contributions
+//                A*dq to its three successors on the next plane through
+//                shared-memory inboxes; the j successor of a chunk's edge
+//                column lives in the neighbouring CTA and is fed through a
+//                ring of planes in that CTA's shared memory.
 #include <algorithm>
 #include <cooperative_groups.h>
 
@@ -270,21 +269,88 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                  : "memory");
 }
 
-constexpr int SWEEP_STAGES = 4;  // ring of staged planes: the current one and three ahead
+constexpr int SWEEP_STAGES = 3;  // ring of staged planes: the current one and two ahead
+constexpr int JRING = 6;         // ring of planes in flight between neighbouring CTAs
+constexpr int SWEEP_COARSE_MAX_THREADS = 384;
+constexpr int SWEEP_FINE_MAX_THREADS = 768;
 
-// shared memory of one CTA with `cpc` column slots: [stages][cpc][SR_N]
-// static records, [stages][cpc][DYN_N] dynamic records, the inbox
-// [2 plane parity][2 dir (j,k)][cpc][10 = A*dq, srv*dq], then the mbarriers
+// shared memory of one CTA with `cpc` column slots:
+//   [SWEEP_STAGES][cpc][SR_N]  static records of a plane
+//   [SWEEP_STAGES][cpc][DYN_N] dynamic records of a plane
+//   [2 plane parity][3 dir (i,j,k)][cpc][10]  inbox from this CTA's own cells
+//   [JRING][cpc][10]           inbox from the neighbouring CTA (j direction)
+//   mbarriers: SWEEP_STAGES (bulk copies), JRING full, JRING empty
 __host__ __device__ inline size_t sweep_smem_bytes(int cpc) {
-    return (size_t)SWEEP_STAGES * cpc * (SR_N + DYN_N) * 8 + (size_t)2 * 2 * cpc * 10 * 8 + SWEEP_STAGES * 8;
+    return (size_t)SWEEP_STAGES * cpc * (SR_N + DYN_N) * 8 + (size_t)2 * 3 * cpc * 10 * 8 + (size_t)JRING * cpc * 10 * 8 +
+           (size_t)(SWEEP_STAGES + 2 * JRING) * 8;
 }
 
-template <int MODE>  // 0 lusgs_l, 1 lusgs_u, 2 gs_pr_l, 3 gs_pr_u
-__global__ void __launch_bounds__(256) k_sweep(DevParams P, PmFields M, const DevBlock *__restrict__ blocks, int *err) {
+__device__ __forceinline__ unsigned remote_u32(const void *local, int rank) {
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smem_u32(local)), "r"(rank));
+    return r;
+}
+// arrive on an mbarrier of another CTA of the cluster without a release
+// fence (the caller orders what must come before it)
+__device__ __forceinline__ void mbar_arrive_remote_relaxed(unsigned cluster_addr) {
+    asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+// stores into another CTA's shared memory, counted as transaction bytes on
+// that CTA's mbarrier
+__device__ __forceinline__ void st_async_v2(unsigned cluster_addr, double a, double b, unsigned cluster_mbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];\n" ::"r"(cluster_addr),
+                 "d"(a), "d"(b), "r"(cluster_mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void st_async_f64(unsigned cluster_addr, double a, unsigned cluster_mbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];\n" ::"r"(cluster_addr), "d"(a),
+                 "r"(cluster_mbar)
+                 : "memory");
+}
+
+// One sweep, one cluster per block, CTA q owning j-chunk q (every chunk at
+// least one column wide).  The work of a cell -- its new dq and the three
+// contributions A*dq for its successors one plane on -- is spread over the
+// lanes of its column:
+//   FINE   16 lanes per column; lane (d, m), d = lane/5, m = lane%5 for
+//          lanes 0..14, evaluates component m of the new dq, receives the
+//          other four from its direction group by warp shuffles, and
+//          evaluates row m of the split Jacobian product along d.
+//   coarse three threads per column (d-major), each evaluating all of dq
+//          and the product along its d (blocks whose chunks are too wide
+//          for FINE).
+// The arithmetic of every value is that of mxdq_std in either layout.  One
+// extra control warp does all mbarrier work, so the compute threads meet
+// nothing but one __syncthreads per plane.
+//
+// Dependencies between CTAs run one way only: in a forward sweep CTA q needs
+// the last column of chunk q-1 from the previous plane, in a backward sweep
+// the first column of chunk q+1.  They travel point to point through a ring
+// of JRING planes in the consumer's shared memory: the producer's boundary
+// threads write 10 values per cell and plane with st.async, whose bytes
+// complete the consumer's `full` mbarrier for that slot (armed by the
+// consumer's control thread with the plane's byte count); once the slot has
+// been read the consumer's control thread re-arms it and arrives on the
+// producer's `empty` mbarrier.  Boundary producers write every plane, inside
+// the block or not, so the byte count per plane is fixed.  No release fence
+// is on the per-plane path, and a CTA may run ahead of its downstream
+// neighbour, so the cross-CTA latency is paid once per chunk rather than
+// once per plane.
+//
+// Per plane pi the control thread, before the CTA's __syncthreads, waits for
+// the bulk copy of plane pi+1, the ring slot holding plane pi-1 (upstream),
+// and the free ring slot for plane pi (downstream); after it, it refills the
+// stage of plane pi with plane pi+SWEEP_STAGES (the compute threads have
+// loaded their coefficients into registers before the barrier) and releases
+// the ring slot read during plane pi-1.
+template <int MODE, bool FINE>  // MODE 0 lusgs_l, 1 lusgs_u, 2 gs_pr_l, 3 gs_pr_u
+__global__ void __launch_bounds__(FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_MAX_THREADS)
+    k_sweep(DevParams P, PmFields M, const DevBlock *__restrict__ blocks, int *err) {
     constexpr bool lu = MODE <= 1;
     constexpr bool with_dyn = MODE != 0;  // lusgs_u: dq of lusgs_l; gs_pr_l/u: old-side terms
     constexpr bool forward = (MODE == 0 || MODE == 2);
     constexpr int step = forward ? 1 : -1;
+    constexpr int NC = FINE ? 1 : 5;  // dq components evaluated per thread
     const int C = M.csize;
     cg::cluster_group cluster = cg::this_cluster();
     const int q = (int)cluster.block_rank();
@@ -297,142 +363,226 @@ __global__ void __launch_bounds__(256) k_sweep(DevParams P, PmFields M, const De
     double *sstat = smem;
     double *sdyn = sstat + (size_t)SWEEP_STAGES * cpc * SR_N;
     double *inbox = sdyn + (size_t)SWEEP_STAGES * cpc * DYN_N;
-    unsigned long long *bars = (unsigned long long *)(inbox + (size_t)2 * 2 * cpc * 10);
-    const size_t inbox_half = (size_t)2 * cpc * 10;
+    double *jring = inbox + (size_t)2 * 3 * cpc * 10;
+    unsigned long long *bars = (unsigned long long *)(jring + (size_t)JRING * cpc * 10);
+    unsigned long long *full = bars + SWEEP_STAGES, *empty = full + JRING;
+    const size_t inbox_half = (size_t)3 * cpc * 10, inbox_dir = (size_t)cpc * 10;
     const int t = threadIdx.x;
-    const bool own = t < ncell;
-    const int k = own ? t / w + 1 : 1;
-    const int j = own ? j0 + t % w + 1 : 1;
-    const int pfirst = forward ? 3 : ni + nj + nk, plast = forward ? ni + nj + nk : 3;
-    // successors of this column along j and k (one step on) receive its contributions
-    const int jn = j + step, kn = k + step;
-    const bool outj = own && jn >= 1 && jn <= nj, outk = own && kn >= 1 && kn <= nk;
-    double *dstj = nullptr, *dstk = nullptr;
-    if (outj) {
-        const int qj = chunk_of(jn - 1, nj, C), j0j = chunk_j0(qj, nj, C), wj = chunk_j0(qj + 1, nj, C) - j0j;
-        double *base = qj == q ? inbox : cluster.map_shared_rank(inbox, qj);
-        dstj = base + (size_t)((k - 1) * wj + (jn - 1 - j0j)) * 10;
-    }
-    if (outk) dstk = inbox + (size_t)cpc * 10 + (size_t)((kn - 1) * w + (j - 1 - j0)) * 10;
-    // predecessors along j and k exist inside the block (at the block faces
-    // the reference multiplies a zero dq: ghost value or the explicit zero of
-    // gs_pr_l/u, so those terms are zero)
+    const bool ctl = t == (int)blockDim.x - 32;  // control thread: lane 0 of the last warp
+    const bool own = FINE ? (t < 16 * ncell && (t & 15) < 15) : t < 3 * ncell;
+    const int d = !own ? 0 : FINE ? (t & 15) / 5 : t / ncell;  // direction of this thread's contribution
+    const int m0 = FINE && own ? (t & 15) % 5 : 0;             // first dq component of this thread
+    const int c = !own ? 0 : FINE ? t >> 4 : t % ncell;        // column within the CTA
+    const int jj = c % w;                                      // column within the chunk
+    const int k = c / w + 1;
+    const int j = j0 + jj + 1;
+    const int pfirst = forward ? 3 : ni + nj + nk;
+    const int nplanes = ni + nj + nk - 2;
+    // neighbouring CTAs: upstream feeds this CTA, downstream is fed by it
+    const int qu = q - step, qd = q + step;
+    const bool has_up = qu >= 0 && qu < C, has_down = qd >= 0 && qd < C;
+    const bool bconsumer = own && has_up && jj == (forward ? 0 : w - 1);
+    const bool bproducer = own && d == 1 && has_down && jj == (forward ? w - 1 : 0);
+    const unsigned ring_bytes = (unsigned)nk * 80u;  // one plane of the boundary column
+    // predecessors along j and k inside the block (at the block faces the
+    // reference multiplies a zero dq: ghost value or the explicit zero of
+    // gs_pr_l/u, so those terms are zero); along i see `hasi` below
     const bool hasj = own && (forward ? j > 1 : j < nj), hask = own && (forward ? k > 1 : k < nk);
+    // destination of this thread's contribution inside the CTA
+    double *dst = nullptr;
+    if (own) {
+        if (d == 0) dst = inbox + (size_t)c * 10;
+        else if (d == 1 && !bproducer && (forward ? j < nj : j > 1)) dst = inbox + inbox_dir + (size_t)(c + step) * 10;
+        else if (d == 2 && (forward ? k < nk : k > 1)) dst = inbox + 2 * inbox_dir + (size_t)(c + step * w) * 10;
+    }
+    const double *srci = inbox + (size_t)c * 10 + m0;
+    const double *srcj = (bconsumer ? jring + (size_t)(k - 1) * 10 : inbox + inbox_dir + (size_t)c * 10) + m0;
+    const double *srck = inbox + 2 * inbox_dir + (size_t)c * 10 + m0;
     const bool vis = lu && P.nvis > 0;
 
-    if (t == 0) {
+    if (ctl) {
         for (int s = 0; s < SWEEP_STAGES; s++) mbar_init(&bars[s], 1);
+        for (int s = 0; s < JRING; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        if (has_up)
+            for (int s = 0; s < JRING; s++) mbar_arrive_expect_tx(&full[s], ring_bytes);
     }
-    __syncthreads();
+    // every CTA's barriers are initialised and armed before anyone writes remotely
+    cluster_arrive();
+    cluster_wait();
+    unsigned ring_remote = 0, full_remote = 0, empty_remote = 0;
+    if (bproducer) {
+        ring_remote = remote_u32(jring + (size_t)(k - 1) * 10, qd);
+        full_remote = remote_u32(full, qd);
+    }
+    if (ctl && has_up) empty_remote = remote_u32(empty, qu);
+
     const unsigned stat_bytes = (unsigned)(ncell * SR_N * 8), dyn_bytes = with_dyn ? (unsigned)(ncell * DYN_N * 8) : 0u;
-    auto issue = [&](int p) {  // thread 0: stage plane p
-        if (ncell == 0 || (forward ? p > plast : p < plast)) return;
-        const int s = ((p - pfirst) * step) % SWEEP_STAGES;
-        const long long pm0 = pmidx(B, p, j0 * nk);
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    auto issue = [&](int pi) {  // control thread: stage plane index pi
+        if (pi >= nplanes) return;
+        const int s = pi % SWEEP_STAGES;
+        const long long pm0 = pmidx(B, pfirst + pi * step, j0 * nk);
         mbar_arrive_expect_tx(&bars[s], stat_bytes + dyn_bytes);
         bulk_g2s(sstat + (size_t)s * cpc * SR_N, M.stat + pm0 * SR_N, stat_bytes, &bars[s]);
         if (with_dyn) bulk_g2s(sdyn + (size_t)s * cpc * DYN_N, M.dyn + pm0 * DYN_N, dyn_bytes, &bars[s]);
     };
-    if (t == 0)
-        for (int a = 0; a < SWEEP_STAGES - 1; a++) issue(pfirst + a * step);
-    // Barrier phases: the arrive after a plane's inbox stores releases them
-    // to the consumers, which wait before reading.  Global stores of dq come
-    // after the arrive (no other CTA reads them in this launch).
-    cluster_arrive();
-
     bool timed_out = false;
-    double cin[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, vin[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // own-column incoming
-    for (int p = pfirst;; p += step) {
+    auto limit = [&]() { return timed_out ? (1LL << 20) : (1LL << 31); };  // ~1 s for the first, then ~0.5 ms
+    if (ctl) {
+        for (int a = 0; a < SWEEP_STAGES; a++) issue(a);
+        if (!mbar_wait(&bars[0], 0u, limit())) timed_out = true;
+    }
+    __syncthreads();
+
+    const double ae = P.gama - 1.0;
+    for (int pi = 0; pi < nplanes; pi++) {
+        const int p = pfirst + pi * step;
         const int i = p - j - k;
         const bool act = own && i >= 1 && i <= ni;
-        const int pi = (p - pfirst) * step;
+        const bool hasi = forward ? i > 1 : i < ni;
         const int s = pi % SWEEP_STAGES;
-        // about a second for the first wait that runs out, then half a millisecond
-        if (ncell > 0 && !mbar_wait(&bars[s], (unsigned)((pi / SWEEP_STAGES) & 1), timed_out ? (1LL << 20) : (1LL << 31)))
-            timed_out = true;
-        cluster_wait();
-        // every thread of this CTA is done with plane p-1: refill its stage
-        if (t == 0) issue(p + (SWEEP_STAGES - 1) * step);
-        double nw[5];
+        // the cell's coefficients (independent of this sweep's new values)
+        double coed = 0.0, base[NC], old0[NC], old1[NC], old2[NC], rv = 0.0, nn = 0.0, uu = 0.0;
+        Jac J;
         if (act) {
-            const double *R = sstat + ((size_t)s * cpc + t) * SR_N;
-            const double *D = sdyn + ((size_t)s * cpc + t) * DYN_N;
-            const double *ib = inbox + (size_t)((p - step) & 1) * inbox_half + (size_t)t * 10;
-            const double *inj = ib, *ink = ib + (size_t)cpc * 10;
-            const double coed = R[SR_COED];
+            const double *R = sstat + ((size_t)s * cpc + c) * SR_N;
+            const double *D = sdyn + ((size_t)s * cpc + c) * DYN_N + m0;
+            coed = R[SR_COED];
 #pragma unroll
-            for (int m = 0; m < 5; m++) {
-                const double cj = hasj ? inj[m] : 0.0, ck = hask ? ink[m] : 0.0;
+            for (int m = 0; m < NC; m++) {
+                base[m] = MODE == 1 ? D[m] : R[SR_RHS + m0 + m];
+                old0[m] = MODE >= 2 ? D[m] : 0.0;
+                old1[m] = MODE == 2 ? D[5 + m] : 0.0;
+                old2[m] = MODE == 2 ? D[10 + m] : 0.0;
+            }
+            J = rec_jac(R, d, forward ? 0 : 1);
+            if (vis) rv = R[SR_SRV + d];
+            if (FINE && m0 > 0) {  // row m0 of the product: (nx, um), (ny, vm), (nz, wm) or (ct, hm)
+                nn = R[SR_JD + 4 * d + (m0 & 3)];
+                uu = R[SR_JS + (m0 == 4 ? 4 : m0 - 1)];
+            }
+        }
+        if (ctl) {
+            if (pi + 1 < nplanes &&
+                !mbar_wait(&bars[(pi + 1) % SWEEP_STAGES], (unsigned)(((pi + 1) / SWEEP_STAGES) & 1), limit()))
+                timed_out = true;
+            // upstream plane pi-1 in ring slot (pi-1) % JRING
+            if (has_up && pi > 0 && !mbar_wait(&full[(pi - 1) % JRING], (unsigned)(((pi - 1) / JRING) & 1), limit()))
+                timed_out = true;
+            // downstream ring slot pi % JRING free (its plane pi - JRING read)
+            if (has_down && pi < nplanes - 1 &&
+                !mbar_wait(&empty[pi % JRING], (unsigned)(((pi / JRING) & 1) ^ 1), limit()))
+                timed_out = true;
+        }
+        __syncthreads();  // own inbox of plane pi-1 complete; coefficients of plane pi in registers
+        if (ctl) {
+            issue(pi + SWEEP_STAGES);
+            if (has_up && pi >= 2) {
+                const int sr = (pi - 2) % JRING;
+                mbar_arrive_expect_tx(&full[sr], ring_bytes);
+                mbar_arrive_remote_relaxed(empty_remote + (unsigned)(sr * 8));
+            }
+        }
+        const size_t rd = (size_t)((pi + 1) & 1) * inbox_half, wr = (size_t)(pi & 1) * inbox_half;
+        // new dq, components m0 .. m0+NC-1
+        double nw[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (act) {
+            const double *inj = srcj + (bconsumer ? (size_t)((pi - 1) % JRING) * cpc * 10 : rd);
+#pragma unroll
+            for (int m = 0; m < NC; m++) {
+                const double ci = hasi ? srci[rd + m] : 0.0, cj = hasj ? inj[m] : 0.0, ck = hask ? srck[rd + m] : 0.0;
                 if (MODE == 0 || MODE == 1) {
-                    const double base = MODE == 0 ? R[SR_RHS + m] : D[m];
-                    double r0 = 1.0 * (cin[m] + cj + ck);
+                    double r0 = 1.0 * (ci + cj + ck);
                     if (vis) {
-                        const double vj = hasj ? inj[5 + m] : 0.0, vk = hask ? ink[5 + m] : 0.0;
-                        const double v = 0.5 * (vin[m] + vj + vk);
+                        const double vi = hasi ? srci[rd + 5 + m] : 0.0, vj = hasj ? inj[5 + m] : 0.0,
+                                     vk = hask ? srck[rd + 5 + m] : 0.0;
+                        const double v = 0.5 * (vi + vj + vk);
                         r0 = MODE == 0 ? r0 + v : r0 - v;
                     }
-                    nw[m] = MODE == 0 ? (-base + r0) * coed : base - r0 * coed;
+                    nw[m] = MODE == 0 ? (-base[m] + r0) * coed : base[m] - r0 * coed;
                 } else if (MODE == 2) {
-                    const double r0 = 1.0 * (cin[m] + cj + ck - D[m] - D[5 + m] - D[10 + m]);
-                    nw[m] = (r0 - R[SR_RHS + m]) * coed;
+                    const double r0 = 1.0 * (ci + cj + ck - old0[m] - old1[m] - old2[m]);
+                    nw[m] = (r0 - base[m]) * coed;
                 } else {
-                    const double r0 = 1.0 * (D[m] - cin[m] - cj - ck);
-                    nw[m] = (r0 - R[SR_RHS + m]) * coed;
+                    const double r0 = 1.0 * (old0[m] - ci - cj - ck);
+                    nw[m] = (r0 - base[m]) * coed;
                 }
             }
-            // this cell's contributions to its successors on the next plane
-            const size_t wb = (size_t)(p & 1) * inbox_half;
+        }
+        const double own_nw = nw[0];  // FINE: component m0
+        if constexpr (FINE) {
+            // gather the five components from the direction group (all lanes take part)
+            const int g = (t & ~15) + 5 * d;
 #pragma unroll
-            for (int d = 0; d < 3; d++) {
-                const Jac J = rec_jac(R, d, forward ? 0 : 1);
-                double o[5];
-                jac_apply(P, J, nw, o);
-                const double rv = vis ? R[SR_SRV + d] : 0.0;
-                if (d == 0) {
+            for (int m = 0; m < 5; m++) nw[m] = __shfl_sync(0xffffffffu, own_nw, (g + m) & 31);
+        }
+        // contribution along d for the successor (rows m0 .. m0+NC-1 of mxdq_std)
+        double o[2 * NC];
+        if (act) {
+            if constexpr (FINE) {
+                const double dc = J.ct * nw[0] - J.nx * nw[1] - J.ny * nw[2] - J.nz * nw[3];
+                const double dh = J.af * nw[0] - ae * (J.um * nw[1] + J.vm * nw[2] + J.wm * nw[3] - nw[4]);
+                const double c2dc = J.c2 * dc;
+                o[0] = m0 == 0 ? J.l1 * nw[0] - dh * J.x1 - dc * J.x2
+                               : J.l1 * own_nw + (nn * c2dc - uu * dh) * J.x1 + (nn * dh - uu * dc) * J.x2;
+                o[1] = rv * own_nw;
+            } else {
+                double f[5];
+                jac_apply(P, J, nw, f);
 #pragma unroll
-                    for (int m = 0; m < 5; m++) {
-                        cin[m] = o[m];
-                        vin[m] = rv * nw[m];
-                    }
-                } else if ((d == 1 && outj) || (d == 2 && outk)) {
-                    double *dst = (d == 1 ? dstj : dstk) + wb;
+                for (int m = 0; m < 5; m++) {
+                    o[m] = f[m];
+                    o[5 + m] = rv * nw[m];
+                }
+            }
+            if (dst) {
 #pragma unroll
-                    for (int m = 0; m < 5; m++) {
-                        dst[m] = o[m];
-                        dst[5 + m] = rv * nw[m];
-                    }
+                for (int m = 0; m < NC; m++) {
+                    dst[wr + m0 + m] = o[m];
+                    dst[wr + 5 + m0 + m] = o[NC + m];
                 }
             }
         } else {
 #pragma unroll
-            for (int m = 0; m < 5; m++) {
-                cin[m] = 0.0;
-                vin[m] = 0.0;
+            for (int m = 0; m < 2 * NC; m++) o[m] = 0.0;  // a boundary producer still sends the plane
+        }
+        if (bproducer && pi < nplanes - 1) {
+            const int so = pi % JRING;
+            const unsigned a = ring_remote + (unsigned)(so * cpc * 80), mb = full_remote + (unsigned)(so * 8);
+            if constexpr (FINE) {
+                st_async_f64(a + 8u * m0, o[0], mb);
+                st_async_f64(a + 8u * (5 + m0), o[1], mb);
+            } else {
+#pragma unroll
+                for (int m = 0; m < 10; m += 2) st_async_v2(a + 8u * m, o[m], o[m + 1], mb);
             }
         }
-        cluster_arrive();
-        if (act) {
-            const long long pm = pmidx(B, p, j0 * nk + t);
+        if (act && d == 0) {
+            const long long pm = pmidx(B, p, j0 * nk + c);
 #pragma unroll
-            for (int m = 0; m < 5; m++) M.dq[m][pm] = nw[m];
+            for (int m = 0; m < NC; m++) M.dq[0][(m0 + m) * M.dq_stride + pm] = FINE ? own_nw : nw[m];
             if (MODE == 0) {
-                double *Dg = M.dyn + pm * DYN_N;  // lusgs_u starts from it
+                double *Dg = M.dyn + pm * DYN_N + m0;  // lusgs_u starts from it
 #pragma unroll
-                for (int m = 0; m < 5; m++) Dg[m] = nw[m];
+                for (int m = 0; m < NC; m++) Dg[m] = FINE ? own_nw : nw[m];
             }
         }
-        if (p == plast) break;
     }
-    // the final wait keeps every CTA alive until the others' remote inbox
-    // stores into it are done; every issued copy has been waited for above
+    // Every issued bulk copy has been waited for above.  Keep every CTA
+    // alive until the others' remote stores and arrivals into it are done:
+    // every ring write has been waited for by its consumer, and the
+    // consumer's arrivals on the producer's `empty` barriers precede the
+    // final barrier.
+    cluster_arrive();
     cluster_wait();
-    if (timed_out && t == 0) atomicAdd(&err[ERR_TIMEOUT], 1);
+    if (timed_out) atomicAdd(&err[ERR_TIMEOUT], 1);
 }
 
-template <int MODE>
-static void launch_sweep(const LaunchCtx &c) {
+template <int MODE, bool FINE>
+static void launch_sweep_t(const LaunchCtx &c) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     cfg.gridDim = dim3(c.nblocks * c.sweep_cluster, 1, 1);
@@ -445,54 +595,75 @@ static void launch_sweep(const LaunchCtx &c) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_sweep<MODE>, *c.P, *c.PM, (const DevBlock *)c.blocks, c.err);
+    cudaLaunchKernelEx(&cfg, k_sweep<MODE, FINE>, *c.P, *c.PM, (const DevBlock *)c.blocks, c.err);
 }
-
 template <int MODE>
-static void sweep_attrs(int smem, bool nonportable) {
-    cudaFuncSetAttribute(k_sweep<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (nonportable) cudaFuncSetAttribute(k_sweep<MODE>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+static void launch_sweep(const LaunchCtx &c) {
+    if (c.sweep_fine) launch_sweep_t<MODE, true>(c);
+    else launch_sweep_t<MODE, false>(c);
 }
 
-// Chooses the cluster size (CTAs per block): the largest power of two <=
-// `cluster` that the hardware can co-schedule with at most 256 column slots
-// and 200 KB of shared memory per CTA.  Returns -1 when nothing fits.
-int setup_sweep(LaunchCtx &c, int cluster) {
-    int maxnj = 0, maxnk = 0;
+template <bool FINE>
+static void sweep_attrs(int smem, bool nonportable) {
+    auto set = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (nonportable) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    };
+    set(k_sweep<0, FINE>);
+    set(k_sweep<1, FINE>);
+    set(k_sweep<2, FINE>);
+    set(k_sweep<3, FINE>);
+}
+
+// Chooses the sweep shape: the lane layout (FINE when `fine` and the chunk
+// fits, else coarse) and the cluster size (CTAs per block), the largest size
+// <= `cluster` and <= the smallest nj (every j-chunk non-empty) that the
+// hardware can co-schedule within the layout's thread limit and 200 KB of
+// shared memory per CTA.  Returns -1 when nothing fits.
+template <bool FINE>
+static bool try_sweep_shape(LaunchCtx &c, int cl, int cpc) {
+    const size_t sm = sweep_smem_bytes(cpc);
+    const int lanes = FINE ? 16 : 3, maxt = FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_MAX_THREADS;
+    const int threads = (lanes * cpc + 31) / 32 * 32 + 32;  // compute warps + the control warp
+    if (threads > maxt || sm > 200 * 1024) return false;
+    sweep_attrs<FINE>((int)sm, cl > 8);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(c.nblocks * cl, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = sm;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, k_sweep<2, FINE>, &cfg);
+    if (e != cudaSuccess || nclusters < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    c.sweep_cluster = cl;
+    c.sweep_cpc = cpc;
+    c.sweep_threads = threads;
+    c.sweep_fine = FINE ? 1 : 0;
+    return true;
+}
+
+int setup_sweep(LaunchCtx &c, int cluster, int fine) {
+    int maxnj = 0, maxnk = 0, minnj = 1 << 30;
     for (int b = 0; b < c.nblocks; b++) {
         maxnj = std::max(maxnj, c.hblocks[b].nj);
         maxnk = std::max(maxnk, c.hblocks[b].nk);
+        minnj = std::min(minnj, c.hblocks[b].nj);
     }
-    for (int cl = std::max(1, std::min(16, cluster)); cl >= 1; cl /= 2) {
-        const int cpc = (maxnj + cl - 1) / cl * maxnk;
-        const size_t sm = sweep_smem_bytes(cpc);
-        if (cpc > 256 || sm > 200 * 1024) continue;
-        const int threads = std::max(32, (cpc + 31) / 32 * 32);
-        sweep_attrs<0>((int)sm, cl > 8);
-        sweep_attrs<1>((int)sm, cl > 8);
-        sweep_attrs<2>((int)sm, cl > 8);
-        sweep_attrs<3>((int)sm, cl > 8);
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute attr[1];
-        cfg.gridDim = dim3(c.nblocks * cl, 1, 1);
-        cfg.blockDim = dim3(threads, 1, 1);
-        cfg.dynamicSmemBytes = sm;
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cl;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        int nclusters = 0;
-        const cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, k_sweep<2>, &cfg);
-        if (e == cudaSuccess && nclusters >= 1) {
-            c.sweep_cluster = cl;
-            c.sweep_cpc = cpc;
-            c.sweep_threads = threads;
-            return 0;
-        }
-        cudaGetLastError();
-    }
+    const int top = std::max(1, std::min(std::min(16, minnj), cluster));
+    if (fine)
+        for (int cl = top; cl >= 1; cl--)
+            if (try_sweep_shape<true>(c, cl, (maxnj + cl - 1) / cl * maxnk)) return 0;
+    for (int cl = top; cl >= 1; cl--)
+        if (try_sweep_shape<false>(c, cl, (maxnj + cl - 1) / cl * maxnk)) return 0;
     return -1;
 }
 

@@ -92,6 +92,7 @@ constexpr int DYN_N = 16;                 // dynamic per-cell record: dq of the 
 
 struct PmFields {
     double *dq[5];   // SoA dq in plane-major order (result of every sweep)
+    long long dq_stride;  // dq[m] = dq[0] + m * dq_stride
     double *stat;    // [cell][SR_N]
     double *dyn;     // [cell][DYN_N]
     int csize;       // CTAs per block cluster (defines the column slots)

@@ -73,7 +73,7 @@ struct LaunchCtx {
     int res_ctas_per_block = 0;
     double *res_out = nullptr;      // per block: res, resmax; then rms
     // LU-SGS sweeps: CTAs per block cluster, columns per CTA, threads per CTA
-    int sweep_cluster = 1, sweep_cpc = 1, sweep_threads = 32;
+    int sweep_cluster = 1, sweep_cpc = 1, sweep_threads = 32, sweep_fine = 0;
     const PmFields *PM = nullptr;  // plane-major sweep arrays
     // update bad-point lists
     int *bad_count = nullptr;       // per block
@@ -92,7 +92,7 @@ void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);
 void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
 void launch_lhs(const LaunchCtx &c);
-int setup_sweep(LaunchCtx &c, int cluster);
+int setup_sweep(LaunchCtx &c, int cluster, int fine);
 void launch_update(const LaunchCtx &c);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
