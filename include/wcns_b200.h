@@ -96,6 +96,28 @@ int wcns_launches_per_step(WcnsContext *ctx);
 /* Number of points shared by more than two blocks (multi-point sets). */
 int wcns_n_multipoints(WcnsContext *ctx);
 
+/* Residual norms of wcns_residual computed from caller-owned device arrays
+ * without allocating any device memory.  No counterpart in the reference:
+ * it exists for callers that may not call cudaMalloc/cudaFree when they need
+ * the residual (a host code whose own pool allocator owns all GPU memory, a
+ * call made from inside another library's callback, a fully committed memory
+ * budget).
+ *   fields: 7*nblocks device pointers, per block dq1..dq5, dtdt, vol, each in
+ *           the ghosted layout above; dims: 3*nblocks (ni, nj, nk >= 3);
+ *   res_per_block, resmax_per_block (nblocks each) and rms: host memory, any
+ *           may be NULL; stream: a cudaStream_t, NULL for the default stream.
+ * The partial sums live in one fixed device array of the library (about
+ * 150 KB, held by every GPU that loads the library until the process exits),
+ * which limits nblocks to WCNS_NOALLOC_MAX_BLOCKS; larger counts are
+ * rejected with WCNS_ERR_ARGUMENT.  The first call on a device looks up that
+ * array's device address, so make it before any stream capture.  Every call
+ * on a device shares the array: calls that overlap on the GPU (other host
+ * threads, other streams) race and must be serialised by the caller.  The
+ * call returns after the results are on the host. */
+#define WCNS_NOALLOC_MAX_BLOCKS 256
+int wcns_residual_noalloc(int nblocks, const int *dims, const double *const *fields, double *res_per_block,
+                          double *resmax_per_block, double *rms, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -30,6 +30,9 @@ using namespace wcns;
 static thread_local std::string g_err;
 static void set_err(const std::string &s) { g_err = s; }
 extern "C" const char *wcns_last_error(void) { return g_err.c_str(); }
+namespace wcns {
+void set_last_error(const std::string &msg) { g_err = msg; }  // for entry points in other files
+}
 
 #define CK(call)                                                                               \
     do {                                                                                       \
