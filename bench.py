@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 METRIC = "Mcell-steps/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # algorithmic bytes per point-step (FP64 words x 8): RHS 20, LU-SGS L 25,
-# U 25, GS-L 30, GS-U 30, update+residual 15 words
+# U 25, GS-L 30, GS-U 30, update+residual 15 words (1,160 B per point-step)
 WORDS = {"rhs": 20, "lhs": 110, "update": 15, "step": 145}
 
 
@@ -136,6 +136,20 @@ def load_peak():
         return 6650.0, "fallback"
 
 
+def load_step_traffic(npoints):
+    """DRAM bytes (read + write) of one time step, summed over the step's
+    kernels from an ncu capture of the plate workload, scaled per point;
+    None when no capture summary is present."""
+    path = os.path.join(ROOT, "profiles", "plate_step_dram.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_point_step:"):
+                return int(float(line.split(":")[1]) * npoints)
+    except OSError:
+        pass
+    return None
+
+
 def make_case(name):
     from wcns_b200 import cases
     if name == "plate":
@@ -212,25 +226,15 @@ def run_b200(args, rank, world):
     total_points = case.npoints * world
     value = total_points * args.steps / (ms / 1e3) / 1e6
 
-    # dominant kernel: the LU-SGS + GS sweeps (l_h_s_tgh without update) timed alone
-    lhs_ms = []
-    for _ in range(5):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        g.boundary_all(); g.initial_q_dq_c_t(); g.timestep_tgh(); g.r_h_s_vis(); g.communicate_dq_npp()
-        g.r_h_s_invis(); g.communicate_dq_npp()
-        e0.record(stream)
-        g.l_h_s_tgh()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        lhs_ms.append(e0.elapsed_time(e1))
-        g.communicate_pv_npp()
-    lhs_avg = statistics.median(lhs_ms)
+    # Roofline of the step program: one graph replay = one step of the whole
+    # path.  Algorithmic bytes = the compulsory traffic of one point-step
+    # (WORDS["step"] FP64 words: each globally dependent phase reads its
+    # inputs once and writes its outputs once) x points; duration = the
+    # CUDA-event time of the timed steps above.
     peak, peak_kind = load_peak()
-    lhs_bytes = case.npoints * (WORDS["lhs"] + WORDS["update"]) * 8
-    achieved = lhs_bytes / (lhs_avg / 1e3) / 1e9
+    step_bytes = case.npoints * WORDS["step"] * 8
+    achieved = step_bytes / (ms / args.steps / 1e3) / 1e9
+    traffic = load_step_traffic(case.npoints)
 
     # end-to-end through the C ABI with pinned host buffers
     pinned = []
@@ -276,11 +280,11 @@ def run_b200(args, rank, world):
                        "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(e2e, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "kernel": "l_h_s_tgh (4 sweeps + update)",
+            "roofline": {"bound": "hbm", "kernel": "one time step (CUDA graph of the whole path)",
                          "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": int(lhs_bytes), "launch_ms": round(lhs_avg, 4),
-                         "traffic": None},
+                         "algorithmic_bytes_per_launch": int(step_bytes), "launch_ms": round(ms / args.steps, 4),
+                         "traffic": traffic},
             "gpu_launches": g.launches_per_step() * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
