@@ -11,10 +11,15 @@
 //   * physical regions: far field (BC.f90:460-607), supersonic inflow
 //     (609-665), supersonic outflow (667-749), viscous wall (1244-1409),
 //     inviscid wall (1412-1486), symmetry (227-457), with dif_average
-//     (1972-2008).  Regions of one block can share edge points, so one CTA per
-//     block walks its regions in order with a barrier between regions.
+//     (1972-2008).  Regions of one block can share edge points, so one
+//     cluster per block walks its regions in order with a cluster barrier
+//     between regions.
+#include <cooperative_groups.h>
+
 #include "wcns_dev.cuh"
 #include "wcns_launch.h"
+
+namespace cg = cooperative_groups;
 
 namespace wcns {
 
@@ -47,9 +52,15 @@ __device__ __forceinline__ void getnxyz(const DevFields &F, long long id, int is
     nz = z / s1;
 }
 
-__global__ void k_bc_physical(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
-                              const DevRegion *__restrict__ regions, const int *__restrict__ reg_first) {
-    const int bi = blockIdx.x;
+// One cluster of BC_CLUSTER CTAs per block: the points of a region are
+// spread over the whole cluster, and a cluster barrier (release/acquire at
+// cluster scope, covering the global-memory writes) separates regions.
+__global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+                                                     const DevRegion *__restrict__ regions,
+                                                     const int *__restrict__ reg_first) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int bi = blockIdx.x / BC_CLUSTER;
+    const int t0 = (int)cluster.block_rank() * blockDim.x + threadIdx.x, tstride = BC_CLUSTER * blockDim.x;
     const DevBlock B = blocks[bi];
     const int r0 = reg_first[bi], r1 = reg_first[bi + 1];
     for (int r = r0; r < r1; r++) {
@@ -74,7 +85,7 @@ __global__ void k_bc_physical(DevParams P, DevFields F, const DevBlock *__restri
                 snz = nz1 / sss1;
             }
         }
-        for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+        for (int t = t0; t < npts; t += tstride) {
             int i = R.s_st[0] + t % e0;
             int j = R.s_st[1] + (t / e0) % e1;
             int k = R.s_st[2] + t / (e0 * e1);
@@ -191,7 +202,7 @@ __global__ void k_bc_physical(DevParams P, DevFields F, const DevBlock *__restri
             default: break;
             }
         }
-        __syncthreads();
+        cluster.sync();
     }
 }
 
@@ -201,7 +212,8 @@ void launch_boundary(const LaunchCtx &c) {
         if (grid > 148 * 16) grid = 148 * 16;
         k_ghost_copy<<<grid, 256, 0, c.stream>>>(*c.F, c.ghost, c.nghost);
     }
-    k_bc_physical<<<c.nblocks, 512, 0, c.stream>>>(*c.P, *c.F, c.blocks, c.regions, c.reg_first);
+    launch_block_clusters(k_bc_physical, c.nblocks, 512, c.stream, *c.P, *c.F, (const DevBlock *)c.blocks,
+                          (const DevRegion *)c.regions, (const int *)c.reg_first);
 }
 
 }  // namespace wcns

@@ -9,8 +9,12 @@
 //   update_limited (Sub2.f90:603-794).
 //   residual_curve (PostProcess.f90:1195-1347).
 //   communicate_dq_npp / communicate_pv_npp (parallel.f90:3020-3326).
+#include <cooperative_groups.h>
+
 #include "wcns_dev.cuh"
 #include "wcns_launch.h"
+
+namespace cg = cooperative_groups;
 
 namespace wcns {
 
@@ -312,13 +316,16 @@ __global__ void k_snapshot(DevFields F, const long long *__restrict__ pts, int n
     }
 }
 
-// boundary_match_dq_2pm / boundary_match_pv_2pm: one CTA per block walks the
-// block's interface regions in region order.
+// boundary_match_dq_2pm / boundary_match_pv_2pm: one cluster per block walks
+// the block's interface regions in region order (cluster barrier between
+// regions: an edge point can belong to two regions).
 __global__ void k_match_2pm(DevFields F, const PairEntry *__restrict__ pairs, const int *__restrict__ blk_reg_first,
                             const int *__restrict__ reg_pair_first, const double *__restrict__ snap, int nsnap, int which) {
-    const int bi = blockIdx.x;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int bi = blockIdx.x / BC_CLUSTER;
+    const int t0 = (int)cluster.block_rank() * blockDim.x + threadIdx.x, tstride = BC_CLUSTER * blockDim.x;
     for (int r = blk_reg_first[bi]; r < blk_reg_first[bi + 1]; r++) {
-        for (int e = reg_pair_first[r] + threadIdx.x; e < reg_pair_first[r + 1]; e += blockDim.x) {
+        for (int e = reg_pair_first[r] + t0; e < reg_pair_first[r + 1]; e += tstride) {
             PairEntry pe = pairs[e];
             if (which == 0) {
                 double vs = F.f[F_VOL][pe.own];
@@ -345,7 +352,7 @@ __global__ void k_match_2pm(DevFields F, const PairEntry *__restrict__ pairs, co
                 }
             }
         }
-        __syncthreads();
+        cluster.sync();
     }
 }
 
@@ -377,7 +384,9 @@ __global__ void k_match_3pp(DevFields F, const int *__restrict__ comp_first, con
 void launch_communicate(const LaunchCtx &c, int which) {
     if (c.nsnap == 0) return;
     k_snapshot<<<(c.nsnap + 255) / 256, 256, 0, c.stream>>>(*c.F, c.snap_pts, c.nsnap, c.snap, which);
-    k_match_2pm<<<c.nblocks, 256, 0, c.stream>>>(*c.F, c.pairs, c.blk_reg_first, c.reg_pair_first, c.snap, c.nsnap, which);
+    launch_block_clusters(k_match_2pm, c.nblocks, 256, c.stream, *c.F, (const PairEntry *)c.pairs,
+                          (const int *)c.blk_reg_first, (const int *)c.reg_pair_first, (const double *)c.snap, c.nsnap,
+                          which);
     if (c.nmem > 0)
         k_match_3pp<<<(c.nmem + 127) / 128, 128, 0, c.stream>>>(*c.F, c.comp_first, c.comp_n, c.mem_slot, c.mem_comp,
                                                              c.mem_idx, c.nmem, c.snap, c.nsnap, which);

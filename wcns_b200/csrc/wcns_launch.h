@@ -82,6 +82,27 @@ struct LaunchCtx {
 
 constexpr int BAD_CAP = 512;
 
+// CTAs per block for the kernels that walk a block's BC or interface
+// regions in order (one cluster per block, cluster barrier between regions)
+constexpr int BC_CLUSTER = 8;
+
+template <class... KArgs, class... Args>
+inline void launch_block_clusters(void (*kern)(KArgs...), int nblocks, int threads, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(nblocks * BC_CLUSTER, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = BC_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 void launch_rhs_invis(const LaunchCtx &c, int dir);
 void setup_rhs_invis_attrs(size_t max_smem);
 void launch_node_derivatives(const LaunchCtx &c);
