@@ -21,13 +21,24 @@
 namespace wcns {
 
 struct InvLine {
-    const double *q[5];  // base pointers (index of point l is (l+2)*stride)
+    const double *sq;  // shared-memory copy of the prim line: sq[m*(n+6) + l+2], l = -2..n+3
+    const double *sk;  // shared-memory copy of the metrics (kx,ky,kz) of the line: sk[c*n + l-1], l = 1..n
     long long stride;
-    long long dqbase;    // field index of point l=0 on the line (point l at dqbase + l*stride)
+    long long dqbase;  // field index of point l=0 on the line (point l at dqbase + l*stride)
     int n, ist, ied;
 };
 
-__device__ __forceinline__ double qv(const InvLine &L, int m, int l) { return __ldg(L.q[m] + (long long)(l + 2) * L.stride); }
+__device__ __forceinline__ double qv(const InvLine &L, int m, int l) { return L.sq[m * (L.n + 6) + l + 2]; }
+
+constexpr int INV_MAX_LINES = 32;  // lines per CTA (short lines are grouped many to a CTA)
+
+// doubles of shared memory per line: prim 5 x (n+6), metrics 3 x n, qwl, qwr,
+// f (5 x (n+1) each) and the 26 boundary-section fluxes; padded to 2 mod 16
+// so that the lines of a group fall on different banks
+__host__ __device__ inline int inv_line_stride(int n) {
+    int raw = 5 * (n + 6) + 3 * n + 15 * (n + 1) + 130;
+    return (raw + 13) / 16 * 16 + 2;
+}
 
 // qwl/qwr after phase B (main value from smem or the 4-style closure)
 __device__ __forceinline__ double qwl_postB(const InvLine &L, const double *sqwl, int m, int h) {
@@ -125,16 +136,19 @@ __device__ __forceinline__ double qwl_preright(const InvLine &L, const double *s
     return qwl_postB(L, sqwl, m, h);
 }
 
+template <int dir>
 __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
-                                                   const LineGroup *__restrict__ groups, int dir, int *err) {
+                                                   const LineGroup *__restrict__ groups, int *err) {
     extern __shared__ double smem[];
     const LineGroup G = groups[blockIdx.x];
     const DevBlock B = blocks[G.blk];
     const int n = dimof(B, dir);
-    const int H = n + 1;
+    const int H = n + 1, W = n + 6;
     const int NL = G.nl;
-    const size_t per_line = (size_t)15 * H + 130;  // qwl, qwr, f (5 x H each) and 26 section fluxes
-    __shared__ InvLine lines[8];
+    const int LS = inv_line_stride(n);
+    // per line: prim, metrics, then qwl, qwr, f (5 x H each) and 26 section fluxes
+    const size_t work0 = (size_t)5 * W + (size_t)3 * n;
+    __shared__ InvLine lines[INV_MAX_LINES];
     const int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
     if (threadIdx.x < NL) {
         int c[3];
@@ -143,7 +157,8 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
         c[dir] = -2;
         long long base = gidx(B, c[0], c[1], c[2]);
         InvLine L;
-        for (int m = 0; m < 5; m++) L.q[m] = F.f[F_R + m] + base;
+        L.sq = smem + (size_t)threadIdx.x * LS;
+        L.sk = L.sq + (size_t)5 * W;
         L.stride = dstride(B, dir);
         L.dqbase = base + 2 * L.stride;
         L.n = n;
@@ -152,7 +167,30 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
         lines[threadIdx.x] = L;
     }
     __syncthreads();
-    const bool posmajor = (dir == 0);
+    constexpr bool posmajor = (dir == 0);
+    // ---- stage the prim line (l = -2..n+3) and the metrics of this
+    // direction (l = 1..n): one thread per (line, point), coalesced along the
+    // line for i-lines and across the group's neighbouring lines otherwise
+    for (int e = threadIdx.x; e < NL * W; e += blockDim.x) {
+        const int ln = posmajor ? e / W : e % NL;
+        const int p = posmajor ? e % W : e / NL;
+        const InvLine &L = lines[ln];
+        const long long gi = L.dqbase + (long long)(p - 2) * L.stride;
+        double v[8];
+#pragma unroll
+        for (int m = 0; m < 5; m++) v[m] = __ldg(F.f[F_R + m] + gi);
+        const bool inner = p >= 3 && p <= n + 2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[5 + c] = inner ? __ldg(F.f[F_KCX + 3 * dir + c] + gi) : 0.0;
+        double *sq = smem + (size_t)ln * LS;
+#pragma unroll
+        for (int m = 0; m < 5; m++) sq[m * W + p] = v[m];
+        if (inner) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) sq[5 * W + c * n + p - 3] = v[5 + c];
+        }
+    }
+    __syncthreads();
     const double CL[3] = {1.0 / 16.0, 10.0 / 16.0, 5.0 / 16.0};
     const double CR[3] = {5.0 / 16.0, 10.0 / 16.0, 1.0 / 16.0};
     const double EPS = 1.0e-6;
@@ -167,7 +205,7 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
             else { ln = idx % NL; m = (idx / NL) % 5; i = idx / (5 * NL); }
             const InvLine &L = lines[ln];
             if (i < L.ist || i > L.ied + 1) continue;
-            double *ql_ = smem + (size_t)ln * per_line;
+            double *ql_ = smem + (size_t)ln * LS + work0;
             double *qr_ = ql_ + (size_t)5 * H;
             double qm2 = qv(L, m, i - 2), qm1 = qv(L, m, i - 1), q0 = qv(L, m, i), qp1 = qv(L, m, i + 1), qp2 = qv(L, m, i + 2);
             double g[3], sdv[3], bl[3], br[3];
@@ -206,7 +244,7 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
             int ln = posmajor ? idx / NT : idx % NL;
             int t = posmajor ? idx % NT : idx / NL;
             const InvLine &L = lines[ln];
-            const double *ql_ = smem + (size_t)ln * per_line;
+            const double *ql_ = smem + (size_t)ln * LS + work0;
             const double *qr_ = ql_ + (size_t)5 * H;
             double ql[5], qr[5], fl[5];
             int h, mode = 0;  // 0 main, 1..6 sections
@@ -257,20 +295,17 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
                 }
             }
             // half-node metrics: VALUE_HALF_NODE of (kx,ky,kz) along the line
-            const double *mx = F.f[F_KCX + 3 * dir] + L.dqbase, *my = F.f[F_KCX + 3 * dir + 1] + L.dqbase,
-                         *mz = F.f[F_KCX + 3 * dir + 2] + L.dqbase;
-            long long st = L.stride;
-            auto ax = [&](int l) { return __ldg(mx + (long long)l * st); };
-            auto ay = [&](int l) { return __ldg(my + (long long)l * st); };
-            auto az = [&](int l) { return __ldg(mz + (long long)l * st); };
+            auto ax = [&](int l) { return L.sk[l - 1]; };
+            auto ay = [&](int l) { return L.sk[n + l - 1]; };
+            auto az = [&](int l) { return L.sk[2 * n + l - 1]; };
             double kx = value_half_node_at(ax, n, h), ky = value_half_node_at(ay, n, h), kz = value_half_node_at(az, n, h);
             const double kt = 0.0;  // kct=0, so every half-node value of kt is +0
             nbad += flux_type(P, ql, qr, kx, ky, kz, kt, fl);
             if (mode == 0) {
-                double *f_ = smem + (size_t)ln * per_line + (size_t)10 * H;
+                double *f_ = smem + (size_t)ln * LS + work0 + (size_t)10 * H;
                 for (int m = 0; m < 5; m++) f_[m * H + h] = fl[m];
             } else {
-                double *sc = smem + (size_t)ln * per_line + (size_t)15 * H + (size_t)(t - H) * 5;
+                double *sc = smem + (size_t)ln * LS + work0 + (size_t)15 * H + (size_t)(t - H) * 5;
                 for (int m = 0; m < 5; m++) sc[m] = fl[m];
             }
         }
@@ -285,8 +320,8 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
             if (posmajor) { l = 1 + idx % n; m = (idx / n) % 5; ln = idx / (5 * n); }
             else { ln = idx % NL; m = (idx / NL) % 5; l = 1 + idx / (5 * NL); }
             const InvLine &L = lines[ln];
-            const double *f_ = smem + (size_t)ln * per_line + (size_t)10 * H;
-            const double *sc = smem + (size_t)ln * per_line + (size_t)15 * H;
+            const double *f_ = smem + (size_t)ln * LS + work0 + (size_t)10 * H;
+            const double *sc = smem + (size_t)ln * LS + work0 + (size_t)15 * H;
             bool right = P.nscheme == 41 && L.ied < n && l >= n - 2;
             bool left = P.nscheme == 41 && L.ist > 1 && l <= 3;
             long long gi = L.dqbase + (long long)l * L.stride;
@@ -315,11 +350,18 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
 void launch_rhs_invis(const LaunchCtx &c, int dir) {
     const DirTable &T = c.inv[dir];
     if (T.ngroups == 0) return;
-    k_rhs_invis<<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, c.err);
+    if (dir == 0) k_rhs_invis<0><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, c.err);
+    else if (dir == 1) k_rhs_invis<1><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, c.err);
+    else k_rhs_invis<2><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, c.err);
 }
 
 void setup_rhs_invis_attrs(size_t max_smem) {
-    cudaFuncSetAttribute(k_rhs_invis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_rhs_invis<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_rhs_invis<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_rhs_invis<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
 }
+
+size_t rhs_invis_line_bytes(int n) { return (size_t)inv_line_stride(n) * 8; }
+int rhs_invis_max_lines() { return INV_MAX_LINES; }
 
 }  // namespace wcns

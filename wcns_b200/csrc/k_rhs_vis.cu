@@ -81,15 +81,32 @@ struct VisLine {
     bool fl, fr;
 };
 
-__global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
-                                                 const LineGroup *__restrict__ groups, int dir, int hmax) {
-    extern __shared__ double smem[];  // fv: NL * 5 * H
+// Shared-memory staging of one line: VIS_NF values per point l = -1 .. n+2
+// (slot l+1): u, v, w, T; the 8 node derivatives along the two other
+// directions; the 9 metrics in the order kcx,etx,ctx,kcy,ety,cty,kcz,etz,ctz;
+// vol; the two Sutherland viscosities.  Then the line's viscous flux, 5 x (n+1).
+constexpr int VIS_NF = 24;
+constexpr int VIS_MAX_LINES = 32;  // lines per CTA (short k-lines are grouped many to a CTA)
+enum : int { VS_U = 0, VS_DN = 4, VS_MET = 12, VS_VOL = 21, VS_V1 = 22, VS_V2 = 23 };
+
+__host__ __device__ inline int vis_line_stride(int n) {
+    // doubles per line, padded to 2 mod 16 so that the lines of a group fall
+    // on different banks when consecutive threads walk consecutive lines
+    int raw = VIS_NF * (n + 4) + 5 * (n + 1);
+    return (raw + 13) / 16 * 16 + 2;
+}
+
+template <int dir>
+__global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+                                                    const LineGroup *__restrict__ groups, int hmax) {
+    extern __shared__ double smem[];
     const LineGroup G = groups[blockIdx.x];
     const DevBlock B = blocks[G.blk];
     const int n = dimof(B, dir);
-    const int H = n + 1;
+    const int H = n + 1, W = n + 4;
     const int NL = G.nl;
-    __shared__ VisLine lines[8];
+    const int LS = vis_line_stride(n);
+    __shared__ VisLine lines[VIS_MAX_LINES];
     const int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
     if (threadIdx.x < NL) {
         int c[3];
@@ -107,17 +124,53 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
     }
     __syncthreads();
     const bool posmajor = (dir == 0);
+    // ---- stage the line inputs: one thread per (line, point), all VIS_NF
+    // loads of the point issued back to back (coalesced along the line for
+    // i-lines, across the group's neighbouring lines otherwise)
+    {
+        const int g0 = dir == 0 ? 1 : 0, g1 = dir == 2 ? 1 : 2;  // the two other directions
+        for (int e = threadIdx.x; e < NL * W; e += blockDim.x) {
+            const int ln = posmajor ? e / W : e % NL;
+            const int p = posmajor ? e % W : e / NL;
+            const VisLine &L = lines[ln];
+            const int l = p - 1;
+            const long long gi = L.l0 + (long long)l * L.st;
+            const bool inner = l >= 1 && l <= n;
+            double v[VIS_NF];
+#pragma unroll
+            for (int m = 0; m < 4; m++) v[VS_U + m] = __ldg(F.f[m == 3 ? F_T : F_U + m] + gi);
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                v[VS_DN + m] = inner ? __ldg(F.f[F_DUV0 + m + 4 * g0] + gi) : 0.0;
+                v[VS_DN + 4 + m] = inner ? __ldg(F.f[F_DUV0 + m + 4 * g1] + gi) : 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < 9; c++)  // kcx,etx,ctx,kcy,... = F_KCX + 3*(c%3) + c/3
+                v[VS_MET + c] = inner ? __ldg(F.f[F_KCX + 3 * (c % 3) + c / 3] + gi) : 0.0;
+            v[VS_VOL] = inner ? __ldg(F.f[F_VOL] + gi) : 0.0;
+            // viscosity at the point, as the reference's visl/vist arrays:
+            // mu + vist and mu*cp_prl + vist*cp_prt with vist = 0 (laminar)
+            const double mu = inner ? sutherland(P, v[VS_U + 3]) : 0.0;
+            v[VS_V1] = inner ? mu + 0.0 : 0.0;
+            v[VS_V2] = inner ? mu * P.cp_prl + 0.0 * P.cp_prt : 0.0;
+            double *S = smem + (size_t)ln * LS + p;
+#pragma unroll
+            for (int f = 0; f < VIS_NF; f++) S[f * W] = v[f];
+        }
+    }
+    __syncthreads();
     // ---- per half node: viscous flux fv
     for (int idx = threadIdx.x; idx < NL * H; idx += blockDim.x) {
         int ln = posmajor ? idx / H : idx % NL;
         int h = posmajor ? idx % H : idx / NL;
         const VisLine &L = lines[ln];
-        const long long l0 = L.l0, st = L.st;
+        const double *S = smem + (size_t)ln * LS;
+        auto at = [&](int f, int x) { return S[f * W + x + 1]; };
         // (u,v,w,T) at the half node: VALUE_line_half_virtual
         double uh[4];
+#pragma unroll
         for (int m = 0; m < 4; m++) {
-            const double *u = F.f[m == 3 ? F_T : F_U + m] + l0;
-            auto Q = [&](int x) { return __ldg(u + (long long)x * st); };
+            auto Q = [&](int x) { return at(VS_U + m, x); };
             double v;
             if (n <= NIJK2ND) v = 0.5 * (Q(h) + Q(h + 1));
             else if (L.fl && h == 0) v = (35.0 * Q(1) + -35.0 * Q(2) + 21.0 * Q(3) + -5.0 * Q(4)) / 16.0;
@@ -130,12 +183,13 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
         // derivatives at the half node: own direction from DUVWT_half_line_virtual,
         // the two others interpolated from node derivatives
         double dh[12];
+#pragma unroll
         for (int g = 0; g < 3; g++) {
+#pragma unroll
             for (int m = 0; m < 4; m++) {
                 double v;
                 if (g == dir) {
-                    const double *u = F.f[m == 3 ? F_T : F_U + m] + l0;
-                    auto Q = [&](int x) { return __ldg(u + (long long)x * st); };
+                    auto Q = [&](int x) { return at(VS_U + m, x); };
                     if (n <= NIJK2ND) v = Q(h + 1) - Q(h);
                     else if (L.fl && h == 0) v = (-71.0 * Q(1) + 141.0 * Q(2) + -93.0 * Q(3) + 23.0 * Q(4)) / 24.0;
                     else if (L.fl && h == 1) v = (-22.0 * Q(1) + 17.0 * Q(2) + 9.0 * Q(3) + -5.0 * Q(4) + 1.0 * Q(5)) / 24.0;
@@ -143,8 +197,8 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
                     else if (L.fr && h == n - 1) v = -(-22.0 * Q(n) + 17.0 * Q(n - 1) + 9.0 * Q(n - 2) + -5.0 * Q(n - 3) + 1.0 * Q(n - 4)) / 24.0;
                     else v = (27.0 * (Q(h + 1) - Q(h)) + -1.0 * (Q(h + 2) - Q(h - 1))) / 24.0;
                 } else {
-                    const double *dn = F.f[F_DUV0 + m + 4 * g] + l0;
-                    auto D = [&](int x) { return __ldg(dn + (long long)x * st); };
+                    const int slot = VS_DN + 4 * (g < dir ? g : g - 1) + m;
+                    auto D = [&](int x) { return at(slot, x); };
                     v = value_half_node_ijk_at(D, n, h);
                 }
                 dh[m + 4 * g] = v;
@@ -152,23 +206,17 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
         }
         // metrics (kcx,etx,ctx,kcy,ety,cty,kcz,etz,ctz), volume, viscosities
         double kh[9];
-        {
-            const int order[9] = {F_KCX, F_ETX, F_CTX, F_KCY, F_ETY, F_CTY, F_KCZ, F_ETZ, F_CTZ};
 #pragma unroll
-            for (int c = 0; c < 9; c++) {
-                const double *a = F.f[order[c]] + l0;
-                auto Q = [&](int x) { return __ldg(a + (long long)x * st); };
-                kh[c] = value_half_node_at(Q, n, h);
-            }
+        for (int c = 0; c < 9; c++) {
+            auto Q = [&](int x) { return at(VS_MET + c, x); };
+            kh[c] = value_half_node_at(Q, n, h);
         }
         double volh, v1h, v2h;
         {
-            const double *a = F.f[F_VOL] + l0;
-            auto Q = [&](int x) { return __ldg(a + (long long)x * st); };
+            auto Q = [&](int x) { return at(VS_VOL, x); };
+            auto V1 = [&](int x) { return at(VS_V1, x); };
+            auto V2 = [&](int x) { return at(VS_V2, x); };
             volh = value_half_node_at(Q, n, h);
-            const double *t = F.f[F_T] + l0;
-            auto V1 = [&](int x) { return sutherland(P, __ldg(t + (long long)x * st)) + 0.0; };
-            auto V2 = [&](int x) { return sutherland(P, __ldg(t + (long long)x * st)) * P.cp_prl + 0.0 * P.cp_prt; };
             v1h = value_half_node_at(V1, n, h);
             v2h = value_half_node_at(V2, n, h);
         }
@@ -195,12 +243,14 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
         double t3 = vs * (dudz + dwdx);
         double t6 = vs * (dvdz + dwdy);
         double kcp = v2h;
-        double nx = kh[dir], ny = kh[dir + 3], nz = kh[dir + 6];
+        const double nx = dir == 0 ? kh[0] : dir == 1 ? kh[1] : kh[2];
+        const double ny = dir == 0 ? kh[3] : dir == 1 ? kh[4] : kh[5];
+        const double nz = dir == 0 ? kh[6] : dir == 1 ? kh[7] : kh[8];
         double f1 = t1 * nx + t2 * ny + t3 * nz;
         double f2 = t2 * nx + t5 * ny + t6 * nz;
         double f3 = t3 * nx + t6 * ny + t9 * nz;
         double f4 = uh[0] * f1 + uh[1] * f2 + uh[2] * f3 + kcp * (dx[9] * nx + dx[10] * ny + dx[11] * nz);
-        double *fv = smem + (size_t)ln * 5 * H;
+        double *fv = smem + (size_t)ln * LS + (size_t)VIS_NF * W;
         fv[0 * H + h] = 0.0;
         fv[1 * H + h] = f1;
         fv[2 * H + h] = f2;
@@ -213,7 +263,7 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
         int ln = posmajor ? idx / n : idx % NL;
         int l = 1 + (posmajor ? idx % n : idx / NL);
         const VisLine &L = lines[ln];
-        const double *fv = smem + (size_t)ln * 5 * H;
+        const double *fv = smem + (size_t)ln * LS + (size_t)VIS_NF * W;
         long long gi = L.l0 + (long long)l * L.st;
 #pragma unroll
         for (int m = 0; m < 5; m++) {
@@ -226,14 +276,21 @@ __global__ void __launch_bounds__(256) k_rhs_vis(DevParams P, DevFields F, const
     (void)hmax;
 }
 
+size_t rhs_vis_line_bytes(int n) { return (size_t)vis_line_stride(n) * 8; }
+int rhs_vis_max_lines() { return VIS_MAX_LINES; }
+
 void launch_rhs_vis(const LaunchCtx &c, int dir) {
     const DirTable &T = c.vis[dir];
     if (T.ngroups == 0) return;
-    k_rhs_vis<<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, dir, T.hmax);
+    if (dir == 0) k_rhs_vis<0><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax);
+    else if (dir == 1) k_rhs_vis<1><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax);
+    else k_rhs_vis<2><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax);
 }
 
 void setup_rhs_vis_attrs(size_t max_smem) {
-    cudaFuncSetAttribute(k_rhs_vis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_rhs_vis<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_rhs_vis<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_rhs_vis<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
 }
 
 }  // namespace wcns

@@ -105,9 +105,13 @@ inline void launch_block_clusters(void (*kern)(KArgs...), int nblocks, int threa
 
 void launch_rhs_invis(const LaunchCtx &c, int dir);
 void setup_rhs_invis_attrs(size_t max_smem);
+size_t rhs_invis_line_bytes(int n);  // shared memory of one line in k_rhs_invis
+int rhs_invis_max_lines();           // lines per CTA in k_rhs_invis
 void launch_node_derivatives(const LaunchCtx &c);
 void launch_rhs_vis(const LaunchCtx &c, int dir);
 void setup_rhs_vis_attrs(size_t max_smem);
+size_t rhs_vis_line_bytes(int n);  // shared memory of one line in k_rhs_vis
+int rhs_vis_max_lines();           // lines per CTA in k_rhs_vis
 void launch_boundary(const LaunchCtx &c);
 void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);
