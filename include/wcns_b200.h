@@ -80,6 +80,12 @@ int wcns_communicate_pv(WcnsContext *ctx);      /* communicate_pv_npp (parallel.
 int wcns_residual(WcnsContext *ctx, double *res_per_block, double *resmax_per_block, double *rms);
                                                 /* residual_curve (PostProcess.f90:1195-1347) */
 
+/* Wall force and moment coefficients: force (PostProcess.f90:1415-1480) with
+ * force_dif / getforce (1505-1824), over all bctype-2 regions.
+ * ref = {sref, lfref, xref, yref, zref, nwholefield} (param.dat $force);
+ * out = {cfx, cfy, cfz, cmx, cmy, cmz, cl, cd, xcp}. */
+int wcns_forces(WcnsContext *ctx, const double *ref, double *out);
+
 /* The whole step of Main.f90:85-109 repeated nsteps times, replayed from a
  * CUDA graph.  rms_history (may be NULL) receives the residual RMS of every
  * step. */

@@ -131,5 +131,13 @@ class Oracle:
             raise RuntimeError(f"oracle step failed ({rc}): " + lib().orc_last_error().decode())
         return hist
 
+    def force(self, sref=1.0, lfref=1.0, xref=0.0, yref=0.0, zref=0.0, nwholefield=1):
+        ref = np.array([sref, lfref, xref, yref, zref, nwholefield], dtype=np.float64)
+        out = np.zeros(9)
+        L = lib()
+        L.orc_forces.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_forces(self.h, ref.ctypes.data, out.ctypes.data)
+        return dict(zip(("cfx", "cfy", "cfz", "cmx", "cmy", "cmz", "cl", "cd", "xcp"), out))
+
     def n_multipoints(self):
         return lib().orc_n_multipoints(self.h)

@@ -65,6 +65,7 @@ typedef struct {
     int nreg;
     Reg *reg;
     int *bcindex;
+    double *xyz[3]; /* grid coordinates, ni*nj*nk each, i fastest (wall forces) */
 } Blk;
 
 typedef struct {
@@ -998,6 +999,14 @@ void *orc_create(const OrcParams *prm, int nblocks, const int *dims, const doubl
     if (analyze_regions(o)) { orc_destroy(o); return NULL; }
     build_multipoints(o);
     for (int nb = 1; nb <= nblocks; nb++) grid_derivative(&o->b[nb], xyz[3 * (nb - 1)], xyz[3 * (nb - 1) + 1], xyz[3 * (nb - 1) + 2]);
+    for (int nb = 1; nb <= nblocks; nb++) {
+        Blk *b = &o->b[nb];
+        size_t np = (size_t)b->ni * b->nj * b->nk;
+        for (int c = 0; c < 3; c++) {
+            b->xyz[c] = malloc(np * sizeof(double));
+            memcpy(b->xyz[c], xyz[3 * (nb - 1) + c], np * sizeof(double));
+        }
+    }
     return o;
 }
 
@@ -1009,6 +1018,7 @@ void orc_destroy(void *h) {
         for (int f = 0; f < F_NFIELDS; f++) free(b->fld[f]);
         for (int m = 0; m < 5; m++) free(b->rhs[m]);
         free(b->vist);
+        for (int c = 0; c < 3; c++) free(b->xyz[c]);
         for (int nr = 0; nr < b->nreg; nr++) { free(b->reg[nr].image); free(b->reg[nr].jmage); free(b->reg[nr].kmage); }
         free(b->reg);
         free(b->bcindex);
@@ -2217,6 +2227,165 @@ int orc_step(void *h, int nsteps, double *rms_history) {
 /* ------------------------------------------------------------------ */
 /* Line-operator hooks for the known-answer tests                      */
 /* ------------------------------------------------------------------ */
+
+/* ------------------------------------------------------------------ */
+/* Wall forces: force (PostProcess.f90:1415-1480), force_dif (1505-1678), */
+/* getforce (1680-1824), getuvwtder (Sub1.f90:383-480), getgeo,          */
+/* getduvwdxyz, stress (Sub1.f90:181-270), aver3/halen/lenth (858-889).  */
+/* ------------------------------------------------------------------ */
+static double lenth(double x1, double y1, double z1, double x2, double y2, double z2) {
+    double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
+    return sqrt(dx * dx + dy * dy + dz * dz);
+}
+static double halen(double a, double b, double c) {
+    double p = 0.5 * (a + b + c);
+    double s = p * (p - a) * (p - b) * (p - c);
+    if (s < 0) return 0.0;
+    return sqrt(s);
+}
+static double aver3(double a, double b, double c) { return (a + b + c) / 3.0; }
+
+static void getforce(const double *px, const double *py, const double *pz, const double *xx, const double *yy,
+                     const double *zz, const double *ref, double *d) {
+    double px5 = 0.25 * (px[0] + px[1] + px[2] + px[3]);
+    double py5 = 0.25 * (py[0] + py[1] + py[2] + py[3]);
+    double pz5 = 0.25 * (pz[0] + pz[1] + pz[2] + pz[3]);
+    double x5 = 0.25 * (xx[0] + xx[1] + xx[2] + xx[3]);
+    double y5 = 0.25 * (yy[0] + yy[1] + yy[2] + yy[3]);
+    double z5 = 0.25 * (zz[0] + zz[1] + zz[2] + zz[3]);
+    double r12 = lenth(xx[0], yy[0], zz[0], xx[1], yy[1], zz[1]);
+    double r23 = lenth(xx[1], yy[1], zz[1], xx[2], yy[2], zz[2]);
+    double r34 = lenth(xx[2], yy[2], zz[2], xx[3], yy[3], zz[3]);
+    double r41 = lenth(xx[3], yy[3], zz[3], xx[0], yy[0], zz[0]);
+    double r15 = lenth(xx[0], yy[0], zz[0], x5, y5, z5);
+    double r25 = lenth(xx[1], yy[1], zz[1], x5, y5, z5);
+    double r35 = lenth(xx[2], yy[2], zz[2], x5, y5, z5);
+    double r45 = lenth(xx[3], yy[3], zz[3], x5, y5, z5);
+    double s[4] = {halen(r12, r15, r25), halen(r23, r25, r35), halen(r34, r35, r45), halen(r41, r45, r15)};
+    double xref = ref[2], yref = ref[3], zref = ref[4];
+    for (int c = 0; c < 6; c++) d[c] = 0.0;
+    for (int t = 0; t < 4; t++) {
+        int a = t, bq = (t + 1) % 4;
+        double pxc = aver3(px[a], px[bq], px5), pyc = aver3(py[a], py[bq], py5), pzc = aver3(pz[a], pz[bq], pz5);
+        double xc = aver3(xx[a], xx[bq], x5), yc = aver3(yy[a], yy[bq], y5), zc = aver3(zz[a], zz[bq], z5);
+        double ddfx = pxc * s[t], ddfy = pyc * s[t], ddfz = pzc * s[t];
+        double ddmx = (yc - yref) * ddfz - (zc - zref) * ddfy;
+        double ddmy = (zc - zref) * ddfx - (xc - xref) * ddfz;
+        double ddmz = (xc - xref) * ddfy - (yc - yref) * ddfx;
+        d[0] = d[0] + ddfx; d[1] = d[1] + ddfy; d[2] = d[2] + ddfz;
+        d[3] = d[3] + ddmx; d[4] = d[4] + ddmy; d[5] = d[5] + ddmz;
+    }
+}
+
+/* surface force per unit-normalised wall point: pressure and, for viscous
+ * runs, the stress tensor from 2nd-order node derivatives */
+static void wall_point_force(const Orc *o, const Blk *b, const Reg *rg, int i, int j, int k, double *pf) {
+    double nx, ny, nz;
+    getnxyz(b, &nx, &ny, &nz, i, j, k, rg->s_lr3d[0], rg->s_lr3d[1], rg->s_lr3d[2]);
+    size_t id = IX(b, i, j, k);
+    double pn = 2.0 * (P(b)[id] - o->poo);
+    double slr = (double)rg->s_lr;
+    pf[0] = slr * nx * pn;
+    pf[1] = slr * ny * pn;
+    pf[2] = slr * nz * pn;
+    if (o->prm.nvis != 1) return;
+    const double *fu[4] = {U(b), V(b), W(b), T(b)};
+    int c[3] = {i, j, k}, dims[3] = {b->ni, b->nj, b->nk};
+    double der[3][4]; /* [direction][u,v,w,t] */
+    for (int d = 0; d < 3; d++) {
+        int e[3] = {0, 0, 0};
+        e[d] = 1;
+        for (int m = 0; m < 4; m++) {
+            const double *f = fu[m];
+            if (c[d] == 1) {
+                double f1 = f[id], f2 = f[IX(b, i + e[0], j + e[1], k + e[2])], f3 = f[IX(b, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2])];
+                der[d][m] = -(1.5 * f1 + -2.0 * f2 + 0.5 * f3);
+            } else if (c[d] == dims[d]) {
+                double f1 = f[id], f2 = f[IX(b, i - e[0], j - e[1], k - e[2])], f3 = f[IX(b, i - 2 * e[0], j - 2 * e[1], k - 2 * e[2])];
+                der[d][m] = 1.5 * f1 + -2.0 * f2 + 0.5 * f3;
+            } else {
+                double fp = f[IX(b, i + e[0], j + e[1], k + e[2])], fm = f[IX(b, i - e[0], j - e[1], k - e[2])];
+                der[d][m] = 0.5 * (fp - fm);
+            }
+        }
+    }
+    double kx = b->fld[F_KCX][id], ky = b->fld[F_KCY][id], kz = b->fld[F_KCZ][id];
+    double ex = b->fld[F_ETX][id], ey = b->fld[F_ETY][id], ez = b->fld[F_ETZ][id];
+    double cx = b->fld[F_CTX][id], cy = b->fld[F_CTY][id], cz = b->fld[F_CTZ][id];
+    double vj = b->fld[F_VOL][id];
+    double dudx = (kx * der[0][0] + ex * der[1][0] + cx * der[2][0]) / vj;
+    double dudy = (ky * der[0][0] + ey * der[1][0] + cy * der[2][0]) / vj;
+    double dudz = (kz * der[0][0] + ez * der[1][0] + cz * der[2][0]) / vj;
+    double dvdx = (kx * der[0][1] + ex * der[1][1] + cx * der[2][1]) / vj;
+    double dvdy = (ky * der[0][1] + ey * der[1][1] + cy * der[2][1]) / vj;
+    double dvdz = (kz * der[0][1] + ez * der[1][1] + cz * der[2][1]) / vj;
+    double dwdx = (kx * der[0][2] + ex * der[1][2] + cx * der[2][2]) / vj;
+    double dwdy = (ky * der[0][2] + ey * der[1][2] + cy * der[2][2]) / vj;
+    double dwdz = (kz * der[0][2] + ez * der[1][2] + cz * der[2][2]) / vj;
+    const double c23 = 0.66666666667;
+    double vis = b->fld[F_VISL][id];
+    double txx = vis * c23 * (2.0 * dudx - dvdy - dwdz);
+    double tyy = vis * c23 * (2.0 * dvdy - dwdz - dudx);
+    double tzz = vis * c23 * (2.0 * dwdz - dudx - dvdy);
+    double txy = vis * (dudy + dvdx);
+    double txz = vis * (dudz + dwdx);
+    double tyz = vis * (dvdz + dwdy);
+    double tyx = txy, tzx = txz, tzy = tyz;
+    double re = 1.0 / o->reynolds;
+    pn = 2.0 * slr;
+    pf[0] = pf[0] - pn * (nx * txx + ny * tyx + nz * tzx) * re;
+    pf[1] = pf[1] - pn * (nx * txy + ny * tyy + nz * tzy) * re;
+    pf[2] = pf[2] - pn * (nx * txz + ny * tyz + nz * tzz) * re;
+}
+
+int orc_forces(void *h, const double *ref, double *out) {
+    Orc *o = h;
+    double cf[6] = {0, 0, 0, 0, 0, 0};
+    for (int nb = 1; nb <= o->nb; nb++) {
+        Blk *b = &o->b[nb];
+        for (int nr = 0; nr < b->nreg; nr++) {
+            Reg *rg = &b->reg[nr];
+            if (!(rg->bctype == 2 || rg->bctype / 10 == 2)) continue;
+            int id_ = 1 - abs(rg->s_lr3d[0]), jd = 1 - abs(rg->s_lr3d[1]), kd = 1 - abs(rg->s_lr3d[2]);
+            int e0 = rg->s_ed[0] - rg->s_st[0] + 1, e1 = rg->s_ed[1] - rg->s_st[1] + 1, e2 = rg->s_ed[2] - rg->s_st[2] + 1;
+            double *pf = malloc(sizeof(double) * 3 * (size_t)e0 * e1 * e2);
+#define PF(i, j, k) (pf + 3 * (size_t)(((i) - rg->s_st[0]) + e0 * (((j) - rg->s_st[1]) + e1 * ((k) - rg->s_st[2]))))
+            for (int i = rg->s_st[0]; i <= rg->s_ed[0]; i++)
+                for (int j = rg->s_st[1]; j <= rg->s_ed[1]; j++)
+                    for (int k = rg->s_st[2]; k <= rg->s_ed[2]; k++) wall_point_force(o, b, rg, i, j, k, PF(i, j, k));
+            for (int i = rg->s_st[0]; i <= rg->s_ed[0] - id_; i++)
+                for (int j = rg->s_st[1]; j <= rg->s_ed[1] - jd; j++)
+                    for (int k = rg->s_st[2]; k <= rg->s_ed[2] - kd; k++) {
+                        int q[4][3] = {{i, j, k}, {0}, {0}, {0}};
+                        if (id_ == 0) { q[1][0] = i; q[1][1] = j + 1; q[1][2] = k; q[2][0] = i; q[2][1] = j + 1; q[2][2] = k + 1; q[3][0] = i; q[3][1] = j; q[3][2] = k + 1; }
+                        if (jd == 0) { q[1][0] = i + 1; q[1][1] = j; q[1][2] = k; q[2][0] = i + 1; q[2][1] = j; q[2][2] = k + 1; q[3][0] = i; q[3][1] = j; q[3][2] = k + 1; }
+                        if (kd == 0) { q[1][0] = i + 1; q[1][1] = j; q[1][2] = k; q[2][0] = i + 1; q[2][1] = j + 1; q[2][2] = k; q[3][0] = i; q[3][1] = j + 1; q[3][2] = k; }
+                        double px[4], py[4], pz[4], xx[4], yy[4], zz[4], d[6];
+                        for (int v = 0; v < 4; v++) {
+                            const double *f = PF(q[v][0], q[v][1], q[v][2]);
+                            px[v] = f[0]; py[v] = f[1]; pz[v] = f[2];
+                            size_t g = (size_t)(q[v][0] - 1) + (size_t)b->ni * ((size_t)(q[v][1] - 1) + (size_t)b->nj * (q[v][2] - 1));
+                            xx[v] = b->xyz[0][g]; yy[v] = b->xyz[1][g]; zz[v] = b->xyz[2][g];
+                        }
+                        getforce(px, py, pz, xx, yy, zz, ref, d);
+                        for (int cc = 0; cc < 6; cc++) cf[cc] = cf[cc] + d[cc];
+                    }
+#undef PF
+            free(pf);
+        }
+    }
+    double sref = ref[0], lfref = ref[1], whole = ref[5];
+    double scf = 1.0 / sref, vcm = 1.0 / (sref * lfref);
+    for (int cc = 0; cc < 3; cc++) out[cc] = (2 - whole) * cf[cc] * scf;
+    for (int cc = 3; cc < 6; cc++) out[cc] = (2 - whole) * cf[cc] * vcm;
+    double attack = o->prm.attack * PAI / 180.0, sideslip = o->prm.sideslip * PAI / 180.0;
+    double sina = sin(attack), cosa = cos(attack), sinb = sin(sideslip), cosb = cos(sideslip);
+    out[6] = out[1] * cosa - out[0] * sina;
+    out[7] = cosb * (out[1] * sina + out[0] * cosa) + sinb * out[2];
+    out[8] = copysign(1.0, out[1]) * out[5] / (fabs(out[1]) + 1.0e-38);
+    return 0;
+}
+
 void orc_value_half_node(int n, int ni, const double *q, double *qh) { value_half_node(n, ni, q, qh); }
 void orc_flux_dxyz(int nl, int ni, const double *f, double *df) { flux_dxyz(nl, ni, f, df); }
 void orc_fluxes(const OrcParams *prm, int nflux, const double *ql, const double *qr, const double *nx4, double *f) {

@@ -51,6 +51,10 @@ int orc_communicate_pv(void *h);
 int orc_residual(void *h, double *res_per_block, double *resmax_per_block, double *rms);
 int orc_step(void *h, int nsteps, double *rms_history);
 int orc_n_multipoints(void *h);
+/* wall forces and moments (force/force_dif/getforce, PostProcess.f90:1415-1824):
+ * ref = {sref, lfref, xref, yref, zref, nwholefield};
+ * out = {cfx, cfy, cfz, cmx, cmy, cmz, cl, cd, xcp} */
+int orc_forces(void *h, const double *ref, double *out);
 
 /* line-operator hooks used by the known-answer tests */
 void orc_value_half_node(int n, int ni, const double *q, double *qh);

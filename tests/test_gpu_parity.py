@@ -107,3 +107,26 @@ def test_graph_step_equals_phase_calls():
     for nb in range(1, case.nblocks + 1):
         for f in PRIM:
             assert np.array_equal(interior(a.get(f, nb), case.dims[nb - 1]), interior(b.get(f, nb), case.dims[nb - 1]))
+
+
+FORCE_REF = dict(sref=2.0, lfref=0.5, xref=0.25, yref=0.0, zref=0.01, nwholefield=1)
+
+
+def test_wall_forces_match_oracle():
+    """force_dif/getforce on the device against the oracle after two steps of
+    the laminar plate: pressure and viscous stress, summed in the reference's
+    loop order (relative to the largest coefficient)."""
+    g, o = make_pair(cases.small_plate_case())
+    g.step(2)
+    o.step(2)
+    fg, fo = g.force(**FORCE_REF), o.force(**FORCE_REF)
+    scale = max(abs(fo[k]) for k in ("cfx", "cfy", "cfz"))
+    for k in ("cfx", "cfy", "cfz", "cmx", "cmy", "cmz", "cl", "cd"):
+        assert abs(fg[k] - fo[k]) <= TOL_PHASE * max(scale, abs(fo[k])), (k, fg[k], fo[k])
+    assert fg["xcp"] == pytest.approx(fo["xcp"], rel=1e-10)
+
+
+def test_no_walls_no_force():
+    g = make_pair(CASES["vortex_sw_4"]())[0]
+    f = g.force()
+    assert all(v == 0.0 for v in f.values())

@@ -145,3 +145,32 @@ def test_freestream_preservation_curved_grid(oracle_lib, nvis, nscheme, nflux):
         if nscheme == 41:
             dq = dq[3:-3, 3:-3, 3:-3]
         assert np.abs(dq).max() <= 1e-11 * area, (m, np.abs(dq).max())
+
+
+def test_force_of_uniform_pressure_on_flat_wall(oracle_lib):
+    """force_dif on the small plate with a uniform excess pressure dp and no
+    viscosity: the wall (y = 0, normal +y, s_lr = -1) carries 2*dp*area in
+    -y, centred at the wall's centroid (PostProcess.f90:1505-1824)."""
+    case = cases.small_plate_case()
+    case.params.nvis = 0
+    o = oracle_lib.Oracle(case)
+    poo = case.params.freestream()[4]
+    dp = 0.1
+    for nb in range(1, len(case.dims) + 1):
+        o.set("p", nb, np.full_like(o.get("p", nb), poo + dp))
+    area, mx, mz = 0.0, 0.0, 0.0
+    for r in case.regions:
+        if r[7] != 2:
+            continue
+        x, y, z = case.xyz[r[0] - 1]
+        sl = tuple(slice(r[2 * d + 1] - 1, r[2 * d + 2]) for d in (2, 1, 0))
+        assert np.abs(y[sl]).max() == 0.0
+        a = (x[sl].max() - x[sl].min()) * (z[sl].max() - z[sl].min())
+        area += a
+        mx += a * 0.5 * (z[sl].max() + z[sl].min())
+        mz += a * 0.5 * (x[sl].max() + x[sl].min())
+    f = o.force(sref=1.0, lfref=1.0)
+    assert f["cfy"] == pytest.approx(-2 * dp * area, rel=1e-13)
+    assert abs(f["cfx"]) < 1e-15 and abs(f["cfz"]) < 1e-15
+    assert f["cmx"] == pytest.approx(2 * dp * mx, rel=1e-12)
+    assert f["cmz"] == pytest.approx(-2 * dp * mz, rel=1e-12)

@@ -42,6 +42,7 @@ SIGNATURES = {
     "wcns_stream": (C.c_void_p, [_VP]),
     "wcns_launches_per_step": (C.c_int, [_VP]),
     "wcns_n_multipoints": (C.c_int, [_VP]),
+    "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
     "wcns_residual_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p), _VP, _VP, _VP, _VP]),
 }
 

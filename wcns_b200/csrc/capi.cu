@@ -13,6 +13,7 @@
 // exchanges between different blocks use start-of-exchange snapshots; a
 // block connected to itself uses the in-place same-rank path.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -607,6 +608,50 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     cudaFree(xyzd);
     cudaFree(work);
     if (e != cudaSuccess) { set_err(std::string("metrics: ") + cudaGetErrorString(e)); delete c; return WCNS_ERR_CUDA; }
+    // wall regions for the force integration, in block and region order
+    {
+        std::vector<DevWall> walls;
+        std::vector<double> wxyz;
+        long long npt = 0, nq = 0;
+        for (int b = 0; b < nblocks; b++)
+            for (const HReg &R : c->blk[b].regs) {
+                if (!(R.bctype == 2 || R.bctype / 10 == 2)) continue;
+                DevWall W{};
+                W.blk = b;
+                int nqr = 1;
+                for (int m = 0; m < 3; m++) {
+                    W.s_st[m] = R.s_st[m];
+                    W.e[m] = R.s_ed[m] - R.s_st[m] + 1;
+                    W.s_lr3d[m] = R.s_lr3d[m];
+                    nqr *= W.e[m] - (1 - std::abs(R.s_lr3d[m]));
+                }
+                W.s_lr = R.s_lr;
+                W.pt_off = npt;
+                W.quad_off = nq;
+                const int ni = c->blk[b].d.ni, nj = c->blk[b].d.nj;
+                for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                    for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                        for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                            size_t g = (size_t)(i - 1) + (size_t)ni * ((size_t)(j - 1) + (size_t)nj * (k - 1));
+                            for (int q = 0; q < 3; q++) wxyz.push_back(xyz[3 * b + q][g]);
+                        }
+                npt += (long long)W.e[0] * W.e[1] * W.e[2];
+                nq += nqr;
+                walls.push_back(W);
+            }
+        L.nwall = (int)walls.size();
+        L.nwall_quads = nq;
+        if (L.nwall) {
+            L.walls = c->up(walls);
+            L.wall_xyz = c->up(wxyz);
+            CK(cudaMalloc(&L.wall_pf, sizeof(double) * 3 * (size_t)npt));
+            c->owned.push_back(L.wall_pf);
+            CK(cudaMalloc(&L.wall_quad, sizeof(double) * 6 * (size_t)std::max(nq, 1LL)));
+            c->owned.push_back(L.wall_quad);
+            CK(cudaMalloc(&L.wall_out, sizeof(double) * 6));
+            c->owned.push_back(L.wall_out);
+        }
+    }
     *out = c;
     return 0;
 }
@@ -692,6 +737,30 @@ extern "C" int wcns_residual(WcnsContext *c, double *res, double *resmax, double
     if (res) std::copy(h.begin(), h.begin() + nb, res);
     if (resmax) std::copy(h.begin() + nb, h.begin() + 2 * nb, resmax);
     if (rms) *rms = h[2 * nb];
+    return 0;
+}
+
+// force (PostProcess.f90:1415-1480): integrate, then normalise on the host
+// as the reference does after its MPI_REDUCE
+extern "C" int wcns_forces(WcnsContext *c, const double *ref, double *out) {
+    if (!c || !ref || !out) { set_err("wcns_forces: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    double cf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (c->L.nwall) {
+        launch_forces(c->L, ref[2], ref[3], ref[4]);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(cf, c->L.wall_out, sizeof cf, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    const double sref = ref[0], lfref = ref[1], whole = ref[5];
+    const double scf = 1.0 / sref, vcm = 1.0 / (sref * lfref);
+    for (int m = 0; m < 3; m++) out[m] = (2 - whole) * cf[m] * scf;
+    for (int m = 3; m < 6; m++) out[m] = (2 - whole) * cf[m] * vcm;
+    const double PAI = 3.14159265;
+    const double attack = c->prm.attack * PAI / 180.0, sideslip = c->prm.sideslip * PAI / 180.0;
+    const double sina = sin(attack), cosa = cos(attack), sinb = sin(sideslip), cosb = cos(sideslip);
+    out[6] = out[1] * cosa - out[0] * sina;
+    out[7] = cosb * (out[1] * sina + out[0] * cosa) + sinb * out[2];
+    out[8] = copysign(1.0, out[1]) * out[5] / (fabs(out[1]) + SMALL);
     return 0;
 }
 

@@ -38,6 +38,7 @@ __global__ void k_init(DevParams P, DevFields F, const DevBlock *__restrict__ bl
         for (int m = 0; m < 5; m++) F.f[F_DQ1 + m][id] = 0.0;
         if (P.nvis != 1) continue;
         t[id] = moo2 * (gama * p[id] / r[id]);
+        F.f[F_VISL][id] = sutherland(P, t[id]);  // compute_visl_ns (GasModel.f90:219-235)
         // ghost layers of the face this point sits on
         int dims[3] = {B.ni, B.nj, B.nk};
         int c[3] = {i, j, k};

@@ -37,6 +37,15 @@ struct PairEntry {
     int same;                // 1 for a block connected to itself
 };
 
+// a wall region for the force integration (bctype 2), in the reference's
+// block and region order
+struct DevWall {
+    int blk;
+    int s_st[3], e[3], s_lr3d[3], s_lr;
+    long long pt_off;    // first point in the wall point arrays
+    long long quad_off;  // first quad in the quad array
+};
+
 struct LaunchCtx {
     cudaStream_t stream = 0;
     const DevParams *P = nullptr;  // host copy, passed by value
@@ -75,6 +84,11 @@ struct LaunchCtx {
     // LU-SGS sweeps: CTAs per block cluster, columns per CTA, threads per CTA
     int sweep_cluster = 1, sweep_cpc = 1, sweep_threads = 32, sweep_fine = 0;
     const PmFields *PM = nullptr;  // plane-major sweep arrays
+    // wall forces
+    DevWall *walls = nullptr;
+    int nwall = 0;
+    long long nwall_quads = 0;
+    double *wall_pf = nullptr, *wall_xyz = nullptr, *wall_quad = nullptr, *wall_out = nullptr;
     // update bad-point lists
     int *bad_count = nullptr;       // per block
     long long *bad_list = nullptr;  // per block, capacity BAD_CAP
@@ -119,6 +133,7 @@ void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
 void launch_lhs(const LaunchCtx &c);
 int setup_sweep(LaunchCtx &c, int cluster, int fine);
 void launch_update(const LaunchCtx &c);
+void launch_forces(const LaunchCtx &c, double xref, double yref, double zref);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
 

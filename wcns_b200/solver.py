@@ -18,6 +18,7 @@ from . import _lib
 FIELDS = ["r", "u", "v", "w", "p", "t", "dq1", "dq2", "dq3", "dq4", "dq5", "dtdt", "sra", "srb", "src",
           "srva", "srvb", "srvc", "kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz", "vol"]
 FID = {n: i for i, n in enumerate(FIELDS)}
+FORCE_KEYS = ("cfx", "cfy", "cfz", "cmx", "cmy", "cmz", "cl", "cd", "xcp")
 
 
 class WcnsError(RuntimeError):
@@ -120,6 +121,14 @@ class Wcns:
         res, rmax, rms = np.zeros(nb), np.zeros(nb), np.zeros(1)
         _check(_lib.load().wcns_residual(self.h, res.ctypes.data, rmax.ctypes.data, rms.ctypes.data))
         return res, rmax, float(rms[0])
+
+    def force(self, sref=1.0, lfref=1.0, xref=0.0, yref=0.0, zref=0.0, nwholefield=1):
+        """Wall force and moment coefficients (force, PostProcess.f90:1415-1480):
+        dict of cfx, cfy, cfz, cmx, cmy, cmz, cl, cd, xcp."""
+        ref = np.array([sref, lfref, xref, yref, zref, nwholefield], dtype=np.float64)
+        out = np.zeros(9)
+        _check(_lib.load().wcns_forces(self.h, ref.ctypes.data, out.ctypes.data))
+        return dict(zip(FORCE_KEYS, out))
 
     def step(self, nsteps=1, history=True):
         """nsteps whole time steps (Main.f90:79-127) replayed from a CUDA graph."""
