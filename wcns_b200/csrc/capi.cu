@@ -437,6 +437,7 @@ static int build_tables(WcnsContext *c) {
     }
     // residual partials, update bad lists
     L.res_ctas_per_block = 32;
+    if (setup_residual(nbk, L.res_ctas_per_block)) { set_err("too many blocks for the residual reduction (at most 400)"); return WCNS_ERR_ARGUMENT; }
     CK(cudaMalloc(&L.res_partial, sizeof(double) * 2 * 32 * nbk));
     c->owned.push_back(L.res_partial);
     CK(cudaMalloc(&L.res_out, sizeof(double) * (2 * nbk + 1)));

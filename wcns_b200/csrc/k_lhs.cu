@@ -113,64 +113,83 @@ __device__ __forceinline__ bool pm_cell(const DevBlock &B, int C, long long q, i
 // prep: for interior neighbours getrkec_mml/getrarbrc return the neighbour's
 // own metrics and spectral radius, so the coefficients depend on the
 // neighbour cell only and are evaluated once per cell.
-__global__ void k_lhs_prep(DevParams P, DevFields F, PmFields M, const DevBlock *__restrict__ blocks) {
+// The records of a CTA's PREP_THREADS consecutive slots are contiguous in
+// memory: each thread builds its record in shared memory, then the CTA
+// writes the whole range with coalesced stores (slots outside the block
+// get zero records).
+constexpr int PREP_THREADS = 128;
+constexpr int PREP_LD = SR_N + 1;  // odd stride: conflict-free record rows
+
+__global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevFields F, PmFields M,
+                                                           const DevBlock *__restrict__ blocks) {
+    __shared__ double srec[PREP_THREADS * PREP_LD];
     const DevBlock B = blocks[blockIdx.y];
     const double gama = P.gama;
     const long long nq = pm_size(B);
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (long long)gridDim.x * blockDim.x) {
+    for (long long q0 = (long long)blockIdx.x * PREP_THREADS; q0 < nq; q0 += (long long)gridDim.x * PREP_THREADS) {
+        const long long q = q0 + threadIdx.x;
+        double *R = srec + threadIdx.x * PREP_LD;
         int i, j, k;
-        if (!pm_cell(B, M.csize, q, i, j, k)) continue;
-        const long long id = gidx(B, i, j, k);
-        const long long pm = B.pmoff + q;
-        double *R = M.stat + pm * SR_N;
-        double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pmr = F.f[F_P][id];
-        double hint = P.g1 * pmr / rm;
-        double c2 = gama * pmr / rm;
-        double cm = sqrt(c2);
-        double v2 = um * um + vm * vm + wm * wm;
-        double hm = hint + 0.5 * v2;
-        double ae = gama - 1.0;
-        R[SR_COED] = F.f[F_COED][id];
+        const bool valid = q < nq && pm_cell(B, M.csize, q, i, j, k);
+        if (!valid) {
+            for (int a = 0; a < SR_N; a++) R[a] = 0.0;
+        } else {
+            const long long id = gidx(B, i, j, k);
+            const long long pm = B.pmoff + q;
+            double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pmr = F.f[F_P][id];
+            double hint = P.g1 * pmr / rm;
+            double c2 = gama * pmr / rm;
+            double cm = sqrt(c2);
+            double v2 = um * um + vm * vm + wm * wm;
+            double hm = hint + 0.5 * v2;
+            double ae = gama - 1.0;
+            R[SR_COED] = F.f[F_COED][id];
 #pragma unroll
-        for (int m = 0; m < 5; m++) {
-            const double v = F.f[F_DQ1 + m][id];
-            R[SR_RHS + m] = v;  // store_rhs_nb (LHS.f90:1592-1613)
-            M.dq[m][pm] = v;
-        }
-        R[SR_JS + 0] = um;
-        R[SR_JS + 1] = vm;
-        R[SR_JS + 2] = wm;
-        R[SR_JS + 3] = c2;
-        R[SR_JS + 4] = hm;
-        R[SR_JS + 5] = 0.5 * ae * v2;
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            double nx = F.f[F_KCX + 3 * d][id], ny = F.f[F_KCX + 3 * d + 1][id], nz = F.f[F_KCX + 3 * d + 2][id], nt = 0.0;
-            double rad = F.f[F_SRA + d][id];
-            double ct = nx * um + ny * vm + nz * wm + nt;
-            double cgm = fmax(sqrt(nx * nx + ny * ny + nz * nz), SML_SSS);
-            double cgm1 = 1.0 / cgm;
-            R[SR_JD + 4 * d + 0] = (ct - nt) * cgm1;
-            R[SR_JD + 4 * d + 1] = nx * cgm1;
-            R[SR_JD + 4 * d + 2] = ny * cgm1;
-            R[SR_JD + 4 * d + 3] = nz * cgm1;
-#pragma unroll
-            for (int sg = 0; sg < 2; sg++) {
-                double dn = sg == 0 ? 1.0 : -1.0;
-                double l1 = ct, l4 = ct + cm * cgm, l5 = ct - cm * cgm;
-                l1 = 0.5 * (l1 + dn * rad);
-                l4 = 0.5 * (l4 + dn * rad);
-                l5 = 0.5 * (l5 + dn * rad);
-                const int b = (sg == 0 ? SR_JP : SR_JM) + 3 * d;
-                R[b + 0] = l1;
-                R[b + 1] = (2.0 * l1 - l4 - l5) / (2.0 * c2);
-                R[b + 2] = (l4 - l5) / (2.0 * cm);
+            for (int m = 0; m < 5; m++) {
+                const double v = F.f[F_DQ1 + m][id];
+                R[SR_RHS + m] = v;  // store_rhs_nb (LHS.f90:1592-1613)
+                M.dq[m][pm] = v;
             }
+            R[SR_JS + 0] = um;
+            R[SR_JS + 1] = vm;
+            R[SR_JS + 2] = wm;
+            R[SR_JS + 3] = c2;
+            R[SR_JS + 4] = hm;
+            R[SR_JS + 5] = 0.5 * ae * v2;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                double nx = F.f[F_KCX + 3 * d][id], ny = F.f[F_KCX + 3 * d + 1][id], nz = F.f[F_KCX + 3 * d + 2][id], nt = 0.0;
+                double rad = F.f[F_SRA + d][id];
+                double ct = nx * um + ny * vm + nz * wm + nt;
+                double cgm = fmax(sqrt(nx * nx + ny * ny + nz * nz), SML_SSS);
+                double cgm1 = 1.0 / cgm;
+                R[SR_JD + 4 * d + 0] = (ct - nt) * cgm1;
+                R[SR_JD + 4 * d + 1] = nx * cgm1;
+                R[SR_JD + 4 * d + 2] = ny * cgm1;
+                R[SR_JD + 4 * d + 3] = nz * cgm1;
+#pragma unroll
+                for (int sg = 0; sg < 2; sg++) {
+                    double dn = sg == 0 ? 1.0 : -1.0;
+                    double l1 = ct, l4 = ct + cm * cgm, l5 = ct - cm * cgm;
+                    l1 = 0.5 * (l1 + dn * rad);
+                    l4 = 0.5 * (l4 + dn * rad);
+                    l5 = 0.5 * (l5 + dn * rad);
+                    const int b = (sg == 0 ? SR_JP : SR_JM) + 3 * d;
+                    R[b + 0] = l1;
+                    R[b + 1] = (2.0 * l1 - l4 - l5) / (2.0 * c2);
+                    R[b + 2] = (l4 - l5) / (2.0 * cm);
+                }
+            }
+            R[SR_SRV + 0] = F.f[F_SRVA][id];
+            R[SR_SRV + 1] = F.f[F_SRVB][id];
+            R[SR_SRV + 2] = F.f[F_SRVC][id];
+            R[SR_N - 1] = 0.0;
         }
-        R[SR_SRV + 0] = F.f[F_SRVA][id];
-        R[SR_SRV + 1] = F.f[F_SRVB][id];
-        R[SR_SRV + 2] = F.f[F_SRVC][id];
-        R[SR_N - 1] = 0.0;
+        __syncthreads();
+        const long long nvalid = nq - q0 < PREP_THREADS ? nq - q0 : PREP_THREADS;
+        double *dst = M.stat + (B.pmoff + q0) * SR_N;
+        for (int e = threadIdx.x; e < nvalid * SR_N; e += PREP_THREADS) dst[e] = srec[(e / SR_N) * PREP_LD + e % SR_N];
+        __syncthreads();
     }
 }
 
@@ -673,7 +692,8 @@ void launch_lhs(const LaunchCtx &c) {
     for (int b = 0; b < c.nblocks; b++) maxp = std::max(maxp, pm_size(c.hblocks[b]));
     const dim3 pg((unsigned)((maxp + 255) / 256), c.nblocks);
     if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
-    k_lhs_prep<<<pg, 256, 0, c.stream>>>(*c.P, *c.F, *c.PM, c.blocks);
+    const dim3 pg128((unsigned)((maxp + PREP_THREADS - 1) / PREP_THREADS), c.nblocks);
+    k_lhs_prep<<<pg128, PREP_THREADS, 0, c.stream>>>(*c.P, *c.F, *c.PM, c.blocks);
     launch_sweep<0>(c);
     launch_sweep<1>(c);
     k_gs_old<2><<<pg, 256, 0, c.stream>>>(*c.P, *c.PM, c.blocks);

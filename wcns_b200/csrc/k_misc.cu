@@ -274,14 +274,20 @@ __global__ void k_residual_partial(DevFields F, const DevBlock *__restrict__ blo
 
 __global__ void k_residual_final(const DevBlock *__restrict__ blocks, int nblocks, const double *partial, int ctas,
                                  double *out, double *rms_slot) {
+    // all partials are fetched in parallel into shared memory first; one
+    // thread then sums them in the fixed order (block by block, CTA by CTA)
+    extern __shared__ double sp[];
+    const int n2 = 2 * nblocks * ctas;
+    for (int e = threadIdx.x; e < n2; e += blockDim.x) sp[e] = partial[e];
+    __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double total = 0.0;
     long long np = 0;
     for (int b = 0; b < nblocks; b++) {
         double s = 0.0, mx = 0.0;
         for (int c = 0; c < ctas; c++) {
-            s = s + partial[2 * ((long long)b * ctas + c)];
-            double m = partial[2 * ((long long)b * ctas + c) + 1];
+            s = s + sp[2 * (b * ctas + c)];
+            double m = sp[2 * (b * ctas + c) + 1];
             mx = m > mx ? m : mx;
         }
         total = total + s;
@@ -295,10 +301,18 @@ __global__ void k_residual_final(const DevBlock *__restrict__ blocks, int nblock
     if (rms_slot) *rms_slot = rms;
 }
 
+int setup_residual(int nblocks, int ctas) {
+    const size_t bytes = sizeof(double) * 2 * (size_t)nblocks * ctas;
+    if (bytes > 200 * 1024) return -1;
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(k_residual_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return 0;
+}
+
 void launch_residual(const LaunchCtx &c, double *rms_slot) {
     dim3 grid(c.res_ctas_per_block, c.nblocks);
     k_residual_partial<<<grid, 256, 0, c.stream>>>(*c.F, c.blocks, c.res_partial, c.res_ctas_per_block);
-    k_residual_final<<<1, 32, 0, c.stream>>>(c.blocks, c.nblocks, c.res_partial, c.res_ctas_per_block, c.res_out, rms_slot);
+    k_residual_final<<<1, 256, sizeof(double) * 2 * c.nblocks * c.res_ctas_per_block, c.stream>>>(
+        c.blocks, c.nblocks, c.res_partial, c.res_ctas_per_block, c.res_out, rms_slot);
 }
 
 // ---------------------------------------------------------------------------

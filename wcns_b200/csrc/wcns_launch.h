@@ -135,6 +135,7 @@ int setup_sweep(LaunchCtx &c, int cluster, int fine);
 void launch_update(const LaunchCtx &c);
 void launch_forces(const LaunchCtx &c, double xref, double yref, double zref);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
+int setup_residual(int nblocks, int ctas);  // -1 when the block count is too large
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
 
 }  // namespace wcns
