@@ -9,7 +9,7 @@ in the last bit, so the bar is a relative error of 1e-12 per field.
 import numpy as np
 import pytest
 
-from tests.helpers import compare_fields, compare_prim_scaled, interior, rel_err
+from tests.helpers import compare_fields, compare_prim_scaled, interior, perturbed, rel_err, supersonic_box_case, with_params
 from wcns_b200 import cases
 
 pytestmark = pytest.mark.gpu
@@ -32,6 +32,13 @@ CASES = {
     "vortex_roe_41": lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=41, nflux=3),
     "plate_small": lambda: cases.small_plate_case(),
     "plate_small_nscheme4_sw": lambda: cases.small_plate_case(nscheme=4, nflux=1),
+    # boundary-condition coverage: adiabatic wall, inviscid wall, 2-D symmetry
+    # (nk <= 4), supersonic inflow/outflow
+    "plate_small_adiabatic": lambda: with_params(cases.small_plate_case(), twall=-1.0),
+    "plate_small_euler_wall": lambda: perturbed(with_params(cases.small_plate_case(nscheme=4, nflux=1), nvis=0)),
+    "plate_small_sym2d": lambda: cases.small_plate_case(nk=4),
+    "supersonic_box_roe41": lambda: supersonic_box_case(),
+    "supersonic_box_sw4": lambda: supersonic_box_case(nscheme=4, nflux=1),
 }
 
 
