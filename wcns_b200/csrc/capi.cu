@@ -98,6 +98,11 @@ struct WcnsContext {
     int launches = 0;
     ~WcnsContext() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (int q = 0; q < 2; q++) {
+            if (L.side[q]) cudaStreamDestroy(L.side[q]);
+            if (L.ev_join[q]) cudaEventDestroy(L.ev_join[q]);
+        }
+        if (L.ev_fork) cudaEventDestroy(L.ev_fork);
         for (void *p : owned) cudaFree(p);
         if (pool) cudaFree(pool);
         if (pm_pool) cudaFree(pm_pool);
@@ -567,6 +572,22 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     for (int b = 0; b < nblocks; b++) hb[b] = c->blk[b].d;
     LaunchCtx &L = c->L;
     L.stream = c->stream;
+    L.total = c->total;
+    for (int q = 0; q < 2; q++) {
+        if (cudaStreamCreateWithFlags(&L.side[q], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&L.ev_join[q], cudaEventDisableTiming) != cudaSuccess) {
+            delete c;
+            set_err("stream/event creation failed");
+            return WCNS_ERR_CUDA;
+        }
+    }
+    if (cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&L.contrib, sizeof(double) * 10 * (size_t)c->total) != cudaSuccess) {
+        delete c;
+        set_err("allocation of the residual contribution buffers failed");
+        return WCNS_ERR_CUDA;
+    }
+    c->owned.push_back(L.contrib);
     L.P = &c->P;
     L.F = &c->F;
     L.PM = &c->PM;
@@ -717,10 +738,10 @@ PHASE(wcns_initial_q_dq_c_t, launch_init(c->L))
 PHASE(wcns_timestep, launch_timestep(c->L))
 PHASE(wcns_rhs_vis, if (c->P.nvis == 1) {
     launch_node_derivatives(c->L);
-    for (int d = 0; d < 3; d++) launch_rhs_vis(c->L, d);
+    launch_rhs_dirs(c->L, true);
 })
 PHASE(wcns_communicate_dq, launch_communicate(c->L, 0))
-PHASE(wcns_rhs_invis, for (int d = 0; d < 3; d++) launch_rhs_invis(c->L, d))
+PHASE(wcns_rhs_invis, launch_rhs_dirs(c->L, false))
 PHASE(wcns_lhs, {
     launch_lhs(c->L);
     launch_update(c->L);
@@ -774,10 +795,14 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     launch_timestep(L); n += 1;
     if (c->P.nvis == 1) {
         launch_node_derivatives(L); n += 1;
-        for (int d = 0; d < 3; d++) { launch_rhs_vis(L, d); n += L.vis[d].ngroups ? 1 : 0; }
+        launch_rhs_dirs(L, true);
+        for (int d = 0; d < 3; d++) n += L.vis[d].ngroups ? 1 : 0;
+        n += (L.vis[1].ngroups || L.vis[2].ngroups) ? 1 : 0;
         launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
     }
-    for (int d = 0; d < 3; d++) { launch_rhs_invis(L, d); n += L.inv[d].ngroups ? 1 : 0; }
+    launch_rhs_dirs(L, false);
+    for (int d = 0; d < 3; d++) n += L.inv[d].ngroups ? 1 : 0;
+    n += (L.inv[1].ngroups || L.inv[2].ngroups) ? 1 : 0;
     launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
     launch_lhs(L); n += 8 + (L.nzero ? 2 : 0);
     launch_update(L); n += 2;

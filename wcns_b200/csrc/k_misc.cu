@@ -301,6 +301,50 @@ __global__ void k_residual_final(const DevBlock *__restrict__ blocks, int nblock
     if (rms_slot) *rms_slot = rms;
 }
 
+// dq -= c1, dq -= c2 (viscous) or dq += c1, dq += c2 (inviscid) over the
+// interior points, after direction 0 updated dq in place: the same sequence
+// of operations as three directions applied one after the other
+__global__ void k_combine_dq(DevFields F, const DevBlock *__restrict__ blocks, const double *__restrict__ c1,
+                             const double *__restrict__ c2, long long stride, int sub) {
+    const DevBlock B = blocks[blockIdx.y];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < B.npts; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode(B, q, i, j, k);
+        const long long id = gidx(B, i, j, k);
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            double v = F.f[F_DQ1 + m][id];
+            if (c1) v = sub ? v - c1[m * stride + id] : v + c1[m * stride + id];
+            if (c2) v = sub ? v - c2[m * stride + id] : v + c2[m * stride + id];
+            F.f[F_DQ1 + m][id] = v;
+        }
+    }
+}
+
+void launch_rhs_dirs(const LaunchCtx &c, bool vis) {
+    const DirTable *T = vis ? c.vis : c.inv;
+    double *out[3] = {nullptr, c.contrib, c.contrib + 5 * c.total};
+    const bool has[3] = {T[0].ngroups > 0, T[1].ngroups > 0, T[2].ngroups > 0};
+    cudaEventRecord(c.ev_fork, c.stream);
+    for (int d = 1; d <= 2; d++) {
+        cudaStreamWaitEvent(c.side[d - 1], c.ev_fork, 0);
+        if (vis) launch_rhs_vis(c, d, c.side[d - 1], out[d]);
+        else launch_rhs_invis(c, d, c.side[d - 1], out[d]);
+        cudaEventRecord(c.ev_join[d - 1], c.side[d - 1]);
+    }
+    if (vis) launch_rhs_vis(c, 0, c.stream, nullptr);
+    else launch_rhs_invis(c, 0, c.stream, nullptr);
+    cudaStreamWaitEvent(c.stream, c.ev_join[0], 0);
+    cudaStreamWaitEvent(c.stream, c.ev_join[1], 0);
+    if (has[1] || has[2]) {
+        long long maxp = 0;
+        for (int b = 0; b < c.nblocks; b++) maxp = c.hblocks[b].npts > maxp ? c.hblocks[b].npts : maxp;
+        dim3 grid((unsigned)((maxp + 255) / 256), c.nblocks);
+        k_combine_dq<<<grid, 256, 0, c.stream>>>(*c.F, c.blocks, has[1] ? out[1] : nullptr, has[2] ? out[2] : nullptr,
+                                                 c.total, vis ? 1 : 0);
+    }
+}
+
 int setup_residual(int nblocks, int ctas) {
     const size_t bytes = sizeof(double) * 2 * (size_t)nblocks * ctas;
     if (bytes > 200 * 1024) return -1;

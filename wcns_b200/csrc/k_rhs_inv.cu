@@ -136,9 +136,12 @@ __device__ __forceinline__ double qwl_preright(const InvLine &L, const double *s
     return qwl_postB(L, sqwl, m, h);
 }
 
+// out == nullptr: dq += dF in place; otherwise dF is stored in
+// out[m*stride + point] for an ordered combine (k_combine_dq)
 template <int dir>
 __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
-                                                   const LineGroup *__restrict__ groups, int *err) {
+                                                   const LineGroup *__restrict__ groups, int *err, double *out,
+                                                   long long stride) {
     extern __shared__ double smem[];
     const LineGroup G = groups[blockIdx.x];
     const DevBlock B = blocks[G.blk];
@@ -341,18 +344,23 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
                 auto fa = [&](int hh) { return f_[m * H + hh]; };
                 df = flux_dxyz_at(fa, n, l);
             }
-            double *dq = F.f[F_DQ1 + m];
-            dq[gi] = dq[gi] + df;
+            if (out) {
+                out[m * stride + gi] = df;
+            } else {
+                double *dq = F.f[F_DQ1 + m];
+                dq[gi] = dq[gi] + df;
+            }
         }
     }
 }
 
-void launch_rhs_invis(const LaunchCtx &c, int dir) {
+void launch_rhs_invis(const LaunchCtx &c, int dir, cudaStream_t st, double *out) {
     const DirTable &T = c.inv[dir];
     if (T.ngroups == 0) return;
-    if (dir == 0) k_rhs_invis<0><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, c.err);
-    else if (dir == 1) k_rhs_invis<1><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, c.err);
-    else k_rhs_invis<2><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, c.err);
+    const long long stride = c.total;
+    if (dir == 0) k_rhs_invis<0><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, c.err, out, stride);
+    else if (dir == 1) k_rhs_invis<1><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, c.err, out, stride);
+    else k_rhs_invis<2><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, c.err, out, stride);
 }
 
 void setup_rhs_invis_attrs(size_t max_smem) {

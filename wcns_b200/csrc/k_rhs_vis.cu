@@ -96,9 +96,12 @@ __host__ __device__ inline int vis_line_stride(int n) {
     return (raw + 13) / 16 * 16 + 2;
 }
 
+// out == nullptr: dq -= re*dFv in place; otherwise re*dFv is stored in
+// out[m*stride + point] for an ordered combine (k_combine_dq)
 template <int dir>
 __global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
-                                                    const LineGroup *__restrict__ groups, int hmax) {
+                                                    const LineGroup *__restrict__ groups, int hmax, double *out,
+                                                    long long stride) {
     extern __shared__ double smem[];
     const LineGroup G = groups[blockIdx.x];
     const DevBlock B = blocks[G.blk];
@@ -269,8 +272,12 @@ __global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, co
         for (int m = 0; m < 5; m++) {
             auto fa = [&](int hh) { return fv[m * H + hh]; };
             double dfv = flux_dxyz_at(fa, n, l);
-            double *dq = F.f[F_DQ1 + m];
-            dq[gi] = dq[gi] - P.re * dfv;
+            if (out) {
+                out[m * stride + gi] = P.re * dfv;
+            } else {
+                double *dq = F.f[F_DQ1 + m];
+                dq[gi] = dq[gi] - P.re * dfv;
+            }
         }
     }
     (void)hmax;
@@ -279,12 +286,13 @@ __global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, co
 size_t rhs_vis_line_bytes(int n) { return (size_t)vis_line_stride(n) * 8; }
 int rhs_vis_max_lines() { return VIS_MAX_LINES; }
 
-void launch_rhs_vis(const LaunchCtx &c, int dir) {
+void launch_rhs_vis(const LaunchCtx &c, int dir, cudaStream_t st, double *out) {
     const DirTable &T = c.vis[dir];
     if (T.ngroups == 0) return;
-    if (dir == 0) k_rhs_vis<0><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax);
-    else if (dir == 1) k_rhs_vis<1><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax);
-    else k_rhs_vis<2><<<T.ngroups, 256, T.smem, c.stream>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax);
+    const long long stride = c.total;
+    if (dir == 0) k_rhs_vis<0><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
+    else if (dir == 1) k_rhs_vis<1><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
+    else k_rhs_vis<2><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
 }
 
 void setup_rhs_vis_attrs(size_t max_smem) {

@@ -48,6 +48,12 @@ struct DevWall {
 
 struct LaunchCtx {
     cudaStream_t stream = 0;
+    long long total = 0;               // points of the field pool (stride of a field)
+    // the three directions of a residual run concurrently: directions 1 and 2
+    // on side streams into contribution buffers, combined in order afterwards
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    double *contrib = nullptr;         // 2 directions x 5 components x total
     const DevParams *P = nullptr;  // host copy, passed by value
     const DevFields *F = nullptr;
     DevBlock *blocks = nullptr;    // device
@@ -117,12 +123,14 @@ inline void launch_block_clusters(void (*kern)(KArgs...), int nblocks, int threa
     cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
-void launch_rhs_invis(const LaunchCtx &c, int dir);
+void launch_rhs_invis(const LaunchCtx &c, int dir, cudaStream_t st, double *out);
 void setup_rhs_invis_attrs(size_t max_smem);
 size_t rhs_invis_line_bytes(int n);  // shared memory of one line in k_rhs_invis
 int rhs_invis_max_lines();           // lines per CTA in k_rhs_invis
 void launch_node_derivatives(const LaunchCtx &c);
-void launch_rhs_vis(const LaunchCtx &c, int dir);
+void launch_rhs_vis(const LaunchCtx &c, int dir, cudaStream_t st, double *out);
+// all three directions of the viscous (vis = true) or inviscid residual
+void launch_rhs_dirs(const LaunchCtx &c, bool vis);
 void setup_rhs_vis_attrs(size_t max_smem);
 size_t rhs_vis_line_bytes(int n);  // shared memory of one line in k_rhs_vis
 int rhs_vis_max_lines();           // lines per CTA in k_rhs_vis
