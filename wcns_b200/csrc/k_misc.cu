@@ -417,26 +417,39 @@ __global__ void k_match_2pm(DevFields F, const PairEntry *__restrict__ pairs, co
 
 // boundary_match_dq_3pp / boundary_match_pv_3pp: points shared by more than
 // two blocks take the mean over all copies (snapshot values, member order).
+// One thread per (field, member copy): the member slots are loaded ahead of
+// the values so that a thread waits on two dependent loads, not on 2*np.
 __global__ void k_match_3pp(DevFields F, const int *__restrict__ comp_first, const int *__restrict__ comp_n,
                             const int *__restrict__ mem_slot, const int *__restrict__ mem_comp,
                             const long long *__restrict__ mem_idx, int nmem, const double *__restrict__ snap,
                             int nsnap, int which) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nmem; e += gridDim.x * blockDim.x) {
-        int c = mem_comp[e];
-        int f0 = comp_first[c], np = comp_n[c];
-        int nf = which == 0 ? 5 : 6;
-        long long id = mem_idx[e];
-        for (int m = 0; m < nf; m++) {
-            double s = 0.0;
-            for (int q = 0; q < np; q++) {
-                double v = snap[(long long)m * nsnap + mem_slot[f0 + q]];
-                if (which == 1) v = v / 1.0;
-                s = s + v;
-            }
-            s = s / (np * 1.0);
-            if (which == 0) F.f[F_DQ1 + m][id] = s * F.f[F_VOL][id];
-            else F.f[F_R + m][id] = s * 1.0;
+    const int nf = which == 0 ? 5 : 6;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf * nmem; t += gridDim.x * blockDim.x) {
+        const int m = t / nmem, e = t - m * nmem;
+        const int c = mem_comp[e];
+        const int f0 = comp_first[c], np = comp_n[c];
+        const long long id = mem_idx[e];
+        const double *sm = snap + (long long)m * nsnap;
+        double s = 0.0;
+        int q = 0;
+        for (; q + 4 <= np; q += 4) {
+            const int s0 = mem_slot[f0 + q], s1 = mem_slot[f0 + q + 1];
+            const int s2 = mem_slot[f0 + q + 2], s3 = mem_slot[f0 + q + 3];
+            double v0 = sm[s0], v1 = sm[s1], v2 = sm[s2], v3 = sm[s3];
+            if (which == 1) { v0 = v0 / 1.0; v1 = v1 / 1.0; v2 = v2 / 1.0; v3 = v3 / 1.0; }
+            s = s + v0;
+            s = s + v1;
+            s = s + v2;
+            s = s + v3;
         }
+        for (; q < np; q++) {
+            double v = sm[mem_slot[f0 + q]];
+            if (which == 1) v = v / 1.0;
+            s = s + v;
+        }
+        s = s / (np * 1.0);
+        if (which == 0) F.f[F_DQ1 + m][id] = s * F.f[F_VOL][id];
+        else F.f[F_R + m][id] = s * 1.0;
     }
 }
 
@@ -447,7 +460,7 @@ void launch_communicate(const LaunchCtx &c, int which) {
                           (const int *)c.blk_reg_first, (const int *)c.reg_pair_first, (const double *)c.snap, c.nsnap,
                           which);
     if (c.nmem > 0)
-        k_match_3pp<<<(c.nmem + 127) / 128, 128, 0, c.stream>>>(*c.F, c.comp_first, c.comp_n, c.mem_slot, c.mem_comp,
+        k_match_3pp<<<((which == 0 ? 5 : 6) * c.nmem + 127) / 128, 128, 0, c.stream>>>(*c.F, c.comp_first, c.comp_n, c.mem_slot, c.mem_comp,
                                                              c.mem_idx, c.nmem, c.snap, c.nsnap, which);
 }
 
