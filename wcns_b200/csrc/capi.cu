@@ -297,13 +297,19 @@ static int build_tables(WcnsContext *c) {
         snap_pts.push_back(id);
         return s;
     };
+    // The reference averages a block's interface points sequentially, region
+    // by region (boundary_match_dq_2pm / boundary_match_pv_2pm).  Each pair
+    // goes to the earliest group (level) after every earlier pair that wrote
+    // its point, wrote the in-block partner it reads, or read its point as a
+    // partner; the pairs of one level are then independent, and running the
+    // levels in order gives the sequential result.
     std::vector<PairEntry> pairs;
     std::vector<int> reg_pair_first, blk_reg_first(nbk + 1, 0);
     for (int b = 0; b < nbk; b++) {
         blk_reg_first[b] = (int)reg_pair_first.size();
+        std::vector<PairEntry> seq;  // the block's pairs in reference order
         for (const HReg &R : c->blk[b].regs) {
             if (R.bctype >= 0) continue;
-            reg_pair_first.push_back((int)pairs.size());
             for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
                 for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
                     for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
@@ -314,8 +320,34 @@ static int build_tables(WcnsContext *c) {
                         slot_of(e.own);
                         e.partner_slot = slot_of(e.partner);
                         e.same = (R.nbt == b + 1) ? 1 : 0;
-                        pairs.push_back(e);
+                        seq.push_back(e);
                     }
+        }
+        std::unordered_map<long long, int> last_write, last_read;
+        std::vector<int> level(seq.size());
+        int nlev = 0;
+        for (size_t a = 0; a < seq.size(); a++) {
+            const PairEntry &e = seq[a];
+            int lv = 0;
+            auto after = [&](const std::unordered_map<long long, int> &mp, long long id) {
+                auto it = mp.find(id);
+                if (it != mp.end()) lv = std::max(lv, it->second + 1);
+            };
+            after(last_write, e.own);
+            after(last_read, e.own);
+            if (e.same) after(last_write, e.partner);
+            level[a] = lv;
+            last_write[e.own] = lv;
+            if (e.same) {
+                auto it = last_read.find(e.partner);
+                last_read[e.partner] = it == last_read.end() ? lv : std::max(it->second, lv);
+            }
+            nlev = std::max(nlev, lv + 1);
+        }
+        for (int lv = 0; lv < nlev; lv++) {
+            reg_pair_first.push_back((int)pairs.size());
+            for (size_t a = 0; a < seq.size(); a++)
+                if (level[a] == lv) pairs.push_back(seq[a]);
         }
     }
     blk_reg_first[nbk] = (int)reg_pair_first.size();

@@ -376,8 +376,9 @@ __global__ void k_snapshot(DevFields F, const long long *__restrict__ pts, int n
 }
 
 // boundary_match_dq_2pm / boundary_match_pv_2pm: one cluster per block walks
-// the block's interface regions in region order (cluster barrier between
-// regions: an edge point can belong to two regions).
+// the block's groups of independent pairs in order, with a cluster barrier
+// between groups (an edge point can belong to two regions; the host puts a
+// pair after every earlier pair it depends on).
 __global__ void k_match_2pm(DevFields F, const PairEntry *__restrict__ pairs, const int *__restrict__ blk_reg_first,
                             const int *__restrict__ reg_pair_first, const double *__restrict__ snap, int nsnap, int which) {
     cg::cluster_group cluster = cg::this_cluster();

@@ -76,8 +76,8 @@ struct LaunchCtx {
     double *snap = nullptr;         // 6 * nsnap
     PairEntry *pairs = nullptr;     // grouped per block, region order
     int *pair_first = nullptr;      // per block (nblocks+1), device
-    int *reg_pair_first = nullptr;  // per block per region boundaries (flattened), device
-    int *blk_reg_first = nullptr;   // per block index into reg_pair_first, device
+    int *reg_pair_first = nullptr;  // per block, boundaries of its groups of independent pairs (flattened), device
+    int *blk_reg_first = nullptr;   // per block, index of its first group in reg_pair_first, device
     int max_pair_regions = 0;
     int ncomp = 0, nmem = 0;
     int *comp_first = nullptr, *comp_n = nullptr, *mem_slot = nullptr;
