@@ -198,14 +198,16 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
     const double CR[3] = {5.0 / 16.0, 10.0 / 16.0, 1.0 / 16.0};
     const double EPS = 1.0e-6;
 
+    // Phases A, B and C walk the items line-fastest in every direction: the lanes
+    // of a warp take the same position on neighbouring lines and follow one
+    // control path, and items without work (boundary sections of a line that
+    // has none) gather into whole warps that skip them.
     // ---- phase A: weights per (line, variable, point i in [ist, ied+1])
     {
         const int NP = n + 2;
         const int nitems = NL * 5 * NP;
         for (int idx = threadIdx.x; idx < nitems; idx += blockDim.x) {
-            int ln, m, i;
-            if (posmajor) { i = idx % NP; m = (idx / NP) % 5; ln = idx / (5 * NP); }
-            else { ln = idx % NL; m = (idx / NL) % 5; i = idx / (5 * NL); }
+            const int ln = idx % NL, m = (idx / NL) % 5, i = idx / (5 * NL);
             const InvLine &L = lines[ln];
             if (i < L.ist || i > L.ied + 1) continue;
             double *ql_ = smem + (size_t)ln * LS + work0;
@@ -244,8 +246,8 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
         const int NT = H + 26;
         int nbad = 0;
         for (int idx = threadIdx.x; idx < NL * NT; idx += blockDim.x) {
-            int ln = posmajor ? idx / NT : idx % NL;
-            int t = posmajor ? idx % NT : idx / NL;
+            const int ln = idx % NL;
+            const int t = idx / NL;
             const InvLine &L = lines[ln];
             const double *ql_ = smem + (size_t)ln * LS + work0;
             const double *qr_ = ql_ + (size_t)5 * H;
@@ -319,9 +321,7 @@ __global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, con
     {
         const int nitems = NL * n * 5;
         for (int idx = threadIdx.x; idx < nitems; idx += blockDim.x) {
-            int ln, l, m;
-            if (posmajor) { l = 1 + idx % n; m = (idx / n) % 5; ln = idx / (5 * n); }
-            else { ln = idx % NL; m = (idx / NL) % 5; l = 1 + idx / (5 * NL); }
+            const int ln = idx % NL, m = (idx / NL) % 5, l = 1 + idx / (5 * NL);
             const InvLine &L = lines[ln];
             const double *f_ = smem + (size_t)ln * LS + work0 + (size_t)10 * H;
             const double *sc = smem + (size_t)ln * LS + work0 + (size_t)15 * H;

@@ -162,10 +162,11 @@ __global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, co
         }
     }
     __syncthreads();
-    // ---- per half node: viscous flux fv
+    // ---- per half node: viscous flux fv (line-fastest in every direction, so
+    // that the lanes of a warp share a position and its control path)
     for (int idx = threadIdx.x; idx < NL * H; idx += blockDim.x) {
-        int ln = posmajor ? idx / H : idx % NL;
-        int h = posmajor ? idx % H : idx / NL;
+        const int ln = idx % NL;
+        const int h = idx / NL;
         const VisLine &L = lines[ln];
         const double *S = smem + (size_t)ln * LS;
         auto at = [&](int f, int x) { return S[f * W + x + 1]; };
@@ -263,8 +264,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, co
     __syncthreads();
     // ---- per point: FLUX_DXYZ and dq -= re*dfv
     for (int idx = threadIdx.x; idx < NL * n; idx += blockDim.x) {
-        int ln = posmajor ? idx / n : idx % NL;
-        int l = 1 + (posmajor ? idx % n : idx / NL);
+        const int ln = idx % NL;
+        const int l = 1 + idx / NL;
         const VisLine &L = lines[ln];
         const double *fv = smem + (size_t)ln * LS + (size_t)VIS_NF * W;
         long long gi = L.l0 + (long long)l * L.st;
