@@ -115,14 +115,16 @@ __device__ __forceinline__ bool pm_cell(const DevBlock &B, int C, long long q, i
 // neighbour cell only and are evaluated once per cell.
 // The records of a CTA's PREP_THREADS consecutive slots are contiguous in
 // memory: each thread builds its record in shared memory, then the CTA
-// writes the whole range with coalesced stores (slots outside the block
-// get zero records).
+// writes the rows of the slots inside the block with coalesced stores.
+// Slots outside the block (about 40% of a plane-major array) keep the zero
+// records they were allocated with: nothing ever writes them.
 constexpr int PREP_THREADS = 128;
 constexpr int PREP_LD = SR_N + 1;  // odd stride: conflict-free record rows
 
 __global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevFields F, PmFields M,
                                                            const DevBlock *__restrict__ blocks) {
     __shared__ double srec[PREP_THREADS * PREP_LD];
+    __shared__ unsigned char srow[PREP_THREADS];  // slot inside the block
     const DevBlock B = blocks[blockIdx.y];
     const double gama = P.gama;
     const long long nq = pm_size(B);
@@ -131,9 +133,8 @@ __global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevField
         double *R = srec + threadIdx.x * PREP_LD;
         int i, j, k;
         const bool valid = q < nq && pm_cell(B, M.csize, q, i, j, k);
-        if (!valid) {
-            for (int a = 0; a < SR_N; a++) R[a] = 0.0;
-        } else {
+        srow[threadIdx.x] = valid ? 1 : 0;
+        if (valid) {
             const long long id = gidx(B, i, j, k);
             const long long pm = B.pmoff + q;
             double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pmr = F.f[F_P][id];
@@ -188,7 +189,10 @@ __global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevField
         __syncthreads();
         const long long nvalid = nq - q0 < PREP_THREADS ? nq - q0 : PREP_THREADS;
         double *dst = M.stat + (B.pmoff + q0) * SR_N;
-        for (int e = threadIdx.x; e < nvalid * SR_N; e += PREP_THREADS) dst[e] = srec[(e / SR_N) * PREP_LD + e % SR_N];
+        for (int e = threadIdx.x; e < nvalid * SR_N; e += PREP_THREADS) {
+            const int r = e / SR_N;
+            if (srow[r]) dst[e] = srec[r * PREP_LD + e - r * SR_N];
+        }
         __syncthreads();
     }
 }
