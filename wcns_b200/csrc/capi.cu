@@ -592,14 +592,17 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     cudaMemset(c->pool, 0, bytes);
     for (int f = 0; f < F_NALL; f++) c->F.f[f] = c->pool + (size_t)f * c->total;
     // sweep arrays, plane-major: dq (5 planes of values), the static records
-    // (SR_N per cell) and the dynamic records (DYN_N per cell)
-    size_t pmbytes = sizeof(double) * (size_t)(5 + SR_N + DYN_N) * (size_t)c->total_pm;
+    // (SR_N per cell) and three dynamic records (DYN_N per cell); the memset
+    // leaves zero the records that no kernel ever writes
+    size_t pmbytes = sizeof(double) * (size_t)(5 + SR_N + 3 * DYN_N) * (size_t)c->total_pm;
     if (cudaMalloc(&c->pm_pool, pmbytes) != cudaSuccess) { delete c; set_err("device allocation of the sweep arrays failed"); return WCNS_ERR_CUDA; }
     cudaMemset(c->pm_pool, 0, pmbytes);
     for (int m = 0; m < 5; m++) c->PM.dq[m] = c->pm_pool + (size_t)m * c->total_pm;
     c->PM.dq_stride = c->total_pm;
     c->PM.stat = c->pm_pool + (size_t)5 * c->total_pm;
     c->PM.dyn = c->PM.stat + (size_t)SR_N * c->total_pm;
+    c->PM.gs[0] = c->PM.dyn + (size_t)DYN_N * c->total_pm;
+    c->PM.gs[1] = c->PM.gs[0] + (size_t)DYN_N * c->total_pm;
     std::vector<DevBlock> hb(nblocks);
     for (int b = 0; b < nblocks; b++) hb[b] = c->blk[b].d;
     LaunchCtx &L = c->L;

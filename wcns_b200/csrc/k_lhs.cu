@@ -16,8 +16,6 @@
 //                acting as a neighbour (both signs, three directions), coed,
 //                the viscous radii -- and rhs = dq (store_rhs_nb), as one
 //                packed 368-byte record per cell in plane-major order.
-//   k_gs_old     (all cells in parallel) the Gauss-Seidel terms of the side
-//                that holds the previous sweep's values.
 //   k_sweep      one thread-block cluster per grid block (the reference's
 //                LU-SGS is block-Jacobi, so blocks are independent).  CTA q
 //                of the cluster owns a j-chunk of the block's (j,k) columns;
@@ -28,7 +26,11 @@
 //                A*dq to its three successors on the next plane through
 //                shared-memory inboxes; the j successor of a chunk's edge
 //                column lives in the neighbouring CTA and is fed through a
-//                ring of planes in that CTA's shared memory.
+//                ring of planes in that CTA's shared memory.  lusgs_u and
+//                gs_pr_l also store these contributions in the successors'
+//                records: evaluated with the sweep's final dq, they are the
+//                Gauss-Seidel terms of the old side that the next sweep
+//                (gs_pr_l, gs_pr_u) reads.
 #include <algorithm>
 #include <cooperative_groups.h>
 
@@ -136,7 +138,6 @@ __global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevField
         srow[threadIdx.x] = valid ? 1 : 0;
         if (valid) {
             const long long id = gidx(B, i, j, k);
-            const long long pm = B.pmoff + q;
             double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pmr = F.f[F_P][id];
             double hint = P.g1 * pmr / rm;
             double c2 = gama * pmr / rm;
@@ -149,7 +150,6 @@ __global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevField
             for (int m = 0; m < 5; m++) {
                 const double v = F.f[F_DQ1 + m][id];
                 R[SR_RHS + m] = v;  // store_rhs_nb (LHS.f90:1592-1613)
-                M.dq[m][pm] = v;
             }
             R[SR_JS + 0] = um;
             R[SR_JS + 1] = vm;
@@ -194,51 +194,6 @@ __global__ void __launch_bounds__(PREP_THREADS) k_lhs_prep(DevParams P, DevField
             if (srow[r]) dst[e] = srec[r * PREP_LD + e - r * SR_N];
         }
         __syncthreads();
-    }
-}
-
-// Gauss-Seidel side holding the previous sweep's values, for all cells:
-// MODE 2 (gs_pr_l) needs the three upper terms der, dfr, dgr separately;
-// MODE 3 (gs_pr_u) needs the lower prefix (del + dfl) + dgl.  A neighbour
-// outside the block has dq = 0 and contributes nothing.
-template <int MODE>
-__global__ void k_gs_old(DevParams P, PmFields M, const DevBlock *__restrict__ blocks) {
-    const DevBlock B = blocks[blockIdx.y];
-    const int C = M.csize;
-    const long long nq = pm_size(B);
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        if (!pm_cell(B, C, q, i, j, k)) continue;
-        const int p = i + j + k;
-        const int cc[3] = {i, j, k}, dims[3] = {B.ni, B.nj, B.nk};
-        constexpr int e = MODE == 2 ? 1 : -1;
-        double term[3][5];
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const bool inside = MODE == 2 ? cc[d] < dims[d] : cc[d] > 1;
-            if (!inside) {
-#pragma unroll
-                for (int m = 0; m < 5; m++) term[d][m] = 0.0;
-                continue;
-            }
-            const int jn = d == 1 ? j + e : j, kn = d == 2 ? k + e : k;
-            const long long npm = pmidx(B, p + e, col_slot(jn, kn, B.nj, B.nk, C));
-            double dn[5];
-#pragma unroll
-            for (int m = 0; m < 5; m++) dn[m] = M.dq[m][npm];
-            Jac J = rec_jac(M.stat + npm * SR_N, d, MODE == 2 ? 1 : 0);
-            jac_apply(P, J, dn, term[d]);
-        }
-        double *D = M.dyn + (B.pmoff + q) * DYN_N;
-        if (MODE == 2) {
-#pragma unroll
-            for (int d = 0; d < 3; d++)
-#pragma unroll
-                for (int m = 0; m < 5; m++) D[5 * d + m] = term[d][m];
-        } else {
-#pragma unroll
-            for (int m = 0; m < 5; m++) D[m] = term[0][m] + term[1][m] + term[2][m];
-        }
     }
 }
 
@@ -444,13 +399,16 @@ __global__ void __launch_bounds__(FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_M
     if (ctl && has_up) empty_remote = remote_u32(empty, qu);
 
     const unsigned stat_bytes = (unsigned)(ncell * SR_N * 8), dyn_bytes = with_dyn ? (unsigned)(ncell * DYN_N * 8) : 0u;
+    // lusgs_u reads the dq of lusgs_l, gs_pr_l / gs_pr_u the old-side terms that
+    // lusgs_u / gs_pr_l left behind
+    const double *dyn_src = MODE == 1 ? M.dyn : MODE == 2 ? M.gs[0] : M.gs[1];
     auto issue = [&](int pi) {  // control thread: stage plane index pi
         if (pi >= nplanes) return;
         const int s = pi % SWEEP_STAGES;
         const long long pm0 = pmidx(B, pfirst + pi * step, j0 * nk);
         mbar_arrive_expect_tx(&bars[s], stat_bytes + dyn_bytes);
         bulk_g2s(sstat + (size_t)s * cpc * SR_N, M.stat + pm0 * SR_N, stat_bytes, &bars[s]);
-        if (with_dyn) bulk_g2s(sdyn + (size_t)s * cpc * DYN_N, M.dyn + pm0 * DYN_N, dyn_bytes, &bars[s]);
+        if (with_dyn) bulk_g2s(sdyn + (size_t)s * cpc * DYN_N, dyn_src + pm0 * DYN_N, dyn_bytes, &bars[s]);
     };
     bool timed_out = false;
     auto limit = [&]() { return timed_out ? (1LL << 20) : (1LL << 31); };  // ~1 s for the first, then ~0.5 ms
@@ -460,6 +418,20 @@ __global__ void __launch_bounds__(FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_M
     }
     __syncthreads();
 
+    // lusgs_u and gs_pr_l: this thread's product along d, evaluated with the
+    // cell's final dq of this sweep, is the old-side term of the successor
+    // along d in the next sweep (what gs_pr_l / gs_pr_u would recompute from
+    // the stored dq); it goes to the successor's record, column slot gs_slot
+    // (plane p + step, column slot gs_slot: gs_rec + (p + step - 3) * one plane)
+    double *gs_rec = nullptr;
+    if ((MODE == 1 || MODE == 2) && own) {
+        int gs_slot = -1;
+        if (d == 0) gs_slot = j0 * nk + c;
+        else if (d == 1 ? (forward ? j < nj : j > 1) : (forward ? k < nk : k > 1))
+            gs_slot = col_slot(d == 1 ? j + step : j, d == 2 ? k + step : k, nj, nk, C);
+        if (gs_slot >= 0) gs_rec = M.gs[MODE == 2 ? 1 : 0] + (B.pmoff + gs_slot) * DYN_N + 5 * d + m0;
+    }
+    const long long gs_plane = (long long)nj * nk * DYN_N;
     const double ae = P.gama - 1.0;
     for (int pi = 0; pi < nplanes; pi++) {
         const int p = pfirst + pi * step;
@@ -477,7 +449,8 @@ __global__ void __launch_bounds__(FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_M
 #pragma unroll
             for (int m = 0; m < NC; m++) {
                 base[m] = MODE == 1 ? D[m] : R[SR_RHS + m0 + m];
-                old0[m] = MODE >= 2 ? D[m] : 0.0;
+                // gs_pr_u: (del + dfl) + dgl of the lower neighbours, gs_pr_l: the three upper terms
+                old0[m] = MODE == 3 ? D[m] + D[5 + m] + D[10 + m] : MODE == 2 ? D[m] : 0.0;
                 old1[m] = MODE == 2 ? D[5 + m] : 0.0;
                 old2[m] = MODE == 2 ? D[10 + m] : 0.0;
             }
@@ -583,10 +556,16 @@ __global__ void __launch_bounds__(FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_M
                 for (int m = 0; m < 10; m += 2) st_async_v2(a + 8u * m, o[m], o[m + 1], mb);
             }
         }
+        if ((MODE == 1 || MODE == 2) && act && gs_rec && (d != 0 || (forward ? i < ni : i > 1))) {
+            double *G = gs_rec + (long long)(p + step - 3) * gs_plane;
+#pragma unroll
+            for (int m = 0; m < NC; m++) G[m] = o[m];
+        }
         if (act && d == 0) {
             const long long pm = pmidx(B, p, j0 * nk + c);
+            if (MODE == 3)  // the result of the four sweeps
 #pragma unroll
-            for (int m = 0; m < NC; m++) M.dq[0][(m0 + m) * M.dq_stride + pm] = FINE ? own_nw : nw[m];
+                for (int m = 0; m < NC; m++) M.dq[0][(m0 + m) * M.dq_stride + pm] = FINE ? own_nw : nw[m];
             if (MODE == 0) {
                 double *Dg = M.dyn + pm * DYN_N + m0;  // lusgs_u starts from it
 #pragma unroll
@@ -700,9 +679,7 @@ void launch_lhs(const LaunchCtx &c) {
     k_lhs_prep<<<pg128, PREP_THREADS, 0, c.stream>>>(*c.P, *c.F, *c.PM, c.blocks);
     launch_sweep<0>(c);
     launch_sweep<1>(c);
-    k_gs_old<2><<<pg, 256, 0, c.stream>>>(*c.P, *c.PM, c.blocks);
     launch_sweep<2>(c);
-    k_gs_old<3><<<pg, 256, 0, c.stream>>>(*c.P, *c.PM, c.blocks);
     launch_sweep<3>(c);
     k_pm_to_std<<<pg, 256, 0, c.stream>>>(*c.F, *c.PM, c.blocks);
     if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);

@@ -88,13 +88,15 @@ enum StatRec : int {
     SR_SRV = 42,                          // srva, srvb, srvc
     SR_N = 46                             // record length (16-byte multiple)
 };
-constexpr int DYN_N = 16;                 // dynamic per-cell record: dq of the previous sweep or old-side terms
+constexpr int DYN_N = 16;                 // dynamic per-cell record: dq of lusgs_l, or old-side terms 5*d + m
 
 struct PmFields {
-    double *dq[5];   // SoA dq in plane-major order (result of every sweep)
+    double *dq[5];   // SoA dq in plane-major order (result of gs_pr_u, the last sweep)
     long long dq_stride;  // dq[m] = dq[0] + m * dq_stride
     double *stat;    // [cell][SR_N]
-    double *dyn;     // [cell][DYN_N]
+    double *dyn;     // [cell][DYN_N] dq of lusgs_l, read by lusgs_u
+    double *gs[2];   // [cell][DYN_N] old-side terms along i, j, k: written by lusgs_u for gs_pr_l (gs[0])
+                     // and by gs_pr_l for gs_pr_u (gs[1]); zero where the neighbour is outside the block
     int csize;       // CTAs per block cluster (defines the column slots)
 };
 
