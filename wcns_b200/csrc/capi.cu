@@ -839,7 +839,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     for (int d = 0; d < 3; d++) n += L.inv[d].ngroups ? 1 : 0;
     n += (L.inv[1].ngroups || L.inv[2].ngroups) ? 1 : 0;
     launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
-    launch_lhs(L); n += 8 + (L.nzero ? 2 : 0);
+    launch_lhs(L); n += 6 + (L.nzero ? 2 : 0);  // prep, four sweeps, plane-major dq to the fields
     launch_update(L); n += 2;
     launch_communicate(L, 1); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
     launch_residual(L, rms_slot); n += 2;
