@@ -259,8 +259,7 @@ def run_b200(args, rank, world):
             g.set_prim(nb, bufs)
         g.step(1, history=False)
         for nb, bufs in enumerate(pinned, start=1):
-            for f, name in enumerate(("r", "u", "v", "w", "p")):
-                g.get(name, nb, out=bufs[f])
+            g.get_prim(nb, out=bufs[:5])
         g.residual_curve()
     e2e_s = time.perf_counter() - t0
     e2e_s = dist_max(e2e_s, world)

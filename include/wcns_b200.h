@@ -66,6 +66,11 @@ const char *wcns_last_error(void);
 int wcns_set_prim(WcnsContext *ctx, int nb, const double *r, const double *u, const double *v, const double *w,
                   const double *p, const double *t);
 int wcns_get_field(WcnsContext *ctx, int field, int nb, double *out);
+/* The primitive state of block nb (r, u, v, w, p, t; t may be NULL) in the
+ * ghosted layout of wcns_set_prim, with one synchronisation for the block:
+ * what the flow-file write reads per block (write_flow_file_parallel,
+ * parallel.f90:4073-4145). */
+int wcns_get_prim(WcnsContext *ctx, int nb, double *r, double *u, double *v, double *w, double *p, double *t);
 int wcns_set_field(WcnsContext *ctx, int field, int nb, const double *in);
 
 /* Per-step drop-ins, in the reference's call order (Main.f90:85-109). */

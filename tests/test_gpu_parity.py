@@ -137,3 +137,18 @@ def test_no_walls_no_force():
     g = make_pair(CASES["vortex_sw_4"]())[0]
     f = g.force()
     assert all(v == 0.0 for v in f.values())
+
+
+def test_get_prim_equals_get_field():
+    """wcns_get_prim returns, block by block, exactly what wcns_get_field
+    returns for r, u, v, w, p, T; with five arrays it leaves T alone."""
+    g = make_pair(cases.small_plate_case())[0]
+    g.step(2)
+    for nb in range(1, len(g.dims) + 1):
+        got = g.get_prim(nb)
+        for a, name in zip(got, ("r", "u", "v", "w", "p", "t")):
+            assert np.array_equal(a, g.get(name, nb)), (nb, name)
+        five = [np.empty_like(a) for a in got[:5]]
+        g.get_prim(nb, out=five)
+        for a, b in zip(five, got[:5]):
+            assert np.array_equal(a, b)

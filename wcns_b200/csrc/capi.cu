@@ -750,6 +750,19 @@ extern "C" int wcns_get_field(WcnsContext *c, int field, int nb, double *out) {
     return 0;
 }
 
+extern "C" int wcns_get_prim(WcnsContext *c, int nb, double *r, double *u, double *v, double *w, double *p, double *t) {
+    const DevBlock *d;
+    if (int rc = block_range(c, nb, &d)) return rc;
+    double *dst[6] = {r, u, v, w, p, t};
+    for (int f = 0; f < 5; f++)
+        if (!dst[f]) { set_err("wcns_get_prim: null array"); return WCNS_ERR_ARGUMENT; }
+    size_t n = (size_t)d->gx * d->gy * d->gz;
+    for (int f = 0; f < 6; f++)
+        if (dst[f]) CK(cudaMemcpyAsync(dst[f], c->F.f[F_R + f] + d->off, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
 extern "C" int wcns_set_field(WcnsContext *c, int field, int nb, const double *in) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;

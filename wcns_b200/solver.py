@@ -87,6 +87,22 @@ class Wcns:
         _check(_lib.load().wcns_get_field(self.h, FID[name], nb, out.ctypes.data))
         return out
 
+    def get_prim(self, nb, out=None):
+        """Copy r, u, v, w, p (and T when `out` has six arrays or is None) of
+        block nb to host memory with one synchronisation; returns the arrays."""
+        ni, nj, nk = self.dims[nb - 1]
+        shape = (nk + 6, nj + 6, ni + 6)
+        if out is None:
+            out = [np.empty(shape) for _ in range(6)]
+        if len(out) not in (5, 6):
+            raise ValueError("get_prim takes five or six output arrays")
+        for a in out:
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("output array has the wrong shape, dtype or layout")
+        ptrs = [a.ctypes.data for a in out] + ([None] if len(out) == 5 else [])
+        _check(_lib.load().wcns_get_prim(self.h, nb, *ptrs))
+        return out
+
     def set(self, name, nb, arr):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
         _check(_lib.load().wcns_set_field(self.h, FID[name], nb, arr.ctypes.data))
