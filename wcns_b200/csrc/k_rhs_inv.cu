@@ -139,7 +139,7 @@ __device__ __forceinline__ double qwl_preright(const InvLine &L, const double *s
 // out == nullptr: dq += dF in place; otherwise dF is stored in
 // out[m*stride + point] for an ordered combine (k_combine_dq)
 template <int dir>
-__global__ void __launch_bounds__(256) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+__global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                    const LineGroup *__restrict__ groups, int *err, double *out,
                                                    long long stride) {
     extern __shared__ double smem[];

@@ -99,7 +99,7 @@ __host__ __device__ inline int vis_line_stride(int n) {
 // out == nullptr: dq -= re*dFv in place; otherwise re*dFv is stored in
 // out[m*stride + point] for an ordered combine (k_combine_dq)
 template <int dir>
-__global__ void __launch_bounds__(256, 2) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+__global__ void __launch_bounds__(256, 3) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                     const LineGroup *__restrict__ groups, int hmax, double *out,
                                                     long long stride) {
     extern __shared__ double smem[];
