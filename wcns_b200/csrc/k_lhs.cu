@@ -95,8 +95,14 @@ __host__ __device__ inline long long pm_size(const DevBlock &B) { return (long l
 // one whose first slot is <= the slot (never an empty chunk).
 __device__ __forceinline__ bool pm_cell(const DevBlock &B, int C, long long q, int &i, int &j, int &k) {
     const int ncol = B.nj * B.nk;
-    const int p = (int)(q / ncol) + 3;
-    const int slot = (int)(q % ncol);
+    int p, slot;
+    if (q < 0x7fffffffLL) {  // 32-bit division where it suffices
+        p = (int)q / ncol + 3;
+        slot = (int)q % ncol;
+    } else {
+        p = (int)(q / ncol) + 3;
+        slot = (int)(q % ncol);
+    }
     int lo = 0, hi = C - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;

@@ -64,7 +64,7 @@ struct DevBlock {
 // contiguous.  Columns are grouped in j-chunks, one chunk per CTA of the
 // block's sweep cluster: chunk q covers j-1 in [q*nj/C, (q+1)*nj/C) for all
 // k, and slot = j0(q)*nk + (k-1)*width(q) + (j-1-j0(q)).
-__host__ __device__ inline int chunk_j0(int q, int nj, int C) { return (int)(((long long)q * nj) / C); }
+__host__ __device__ inline int chunk_j0(int q, int nj, int C) { return q * nj / C; }  // q <= C <= 16: no overflow
 __host__ __device__ inline int chunk_of(int jj, int nj, int C) {  // jj = j-1
     int q = (int)(((long long)jj * C) / nj);
     if (q > C - 1) q = C - 1;
