@@ -18,11 +18,7 @@ namespace cg = cooperative_groups;
 
 namespace wcns {
 
-__device__ __forceinline__ void decode(const DevBlock &B, long long p, int &i, int &j, int &k) {
-    i = (int)(p % B.ni) + 1;
-    j = (int)((p / B.ni) % B.nj) + 1;
-    k = (int)(p / ((long long)B.ni * B.nj)) + 1;
-}
+__device__ __forceinline__ void decode(const DevBlock &B, long long p, int &i, int &j, int &k) { decode_point(B, p, i, j, k); }
 
 // ---------------------------------------------------------------------------
 __global__ void k_init(DevParams P, DevFields F, const DevBlock *__restrict__ blocks, int nblocks) {

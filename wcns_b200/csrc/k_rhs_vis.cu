@@ -22,15 +22,14 @@ namespace wcns {
 // ---------------------------------------------------------------------------
 // node derivatives: one thread per interior point
 // ---------------------------------------------------------------------------
-__global__ void k_node_deriv(DevParams P, DevFields F, const DevBlock *__restrict__ blocks, int nblocks) {
+__global__ void __launch_bounds__(256, 4) k_node_deriv(DevParams P, DevFields F, const DevBlock *__restrict__ blocks, int nblocks) {
     int bi = blockIdx.y;
     if (bi >= nblocks) return;
     const DevBlock B = blocks[bi];
     long long np = B.npts;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(p % B.ni) + 1;
-        int j = (int)((p / B.ni) % B.nj) + 1;
-        int k = (int)(p / ((long long)B.ni * B.nj)) + 1;
+        int i, j, k;
+        decode_point(B, p, i, j, k);
         long long id = gidx(B, i, j, k);
         for (int d = 0; d < 3; d++) {
             int n = dimof(B, d);

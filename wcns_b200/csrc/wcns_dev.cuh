@@ -112,6 +112,21 @@ __host__ __device__ inline long long gidx(const DevBlock &b, int i, int j, int k
     return b.off + (long long)(i + 2) + (long long)b.gx * ((long long)(j + 2) + (long long)b.gy * (long long)(k + 2));
 }
 
+// interior point index p = (i-1) + ni*((j-1) + nj*(k-1)) -> (i, j, k); 32-bit
+// divisions whenever p fits (every realistic block)
+__device__ __forceinline__ void decode_point(const DevBlock &B, long long p, int &i, int &j, int &k) {
+    if (p < 0x7fffffffLL) {
+        const int q = (int)p, r = q / B.ni;
+        i = q - r * B.ni + 1;
+        j = r % B.nj + 1;
+        k = r / B.nj + 1;
+    } else {
+        i = (int)(p % B.ni) + 1;
+        j = (int)((p / B.ni) % B.nj) + 1;
+        k = (int)(p / ((long long)B.ni * B.nj)) + 1;
+    }
+}
+
 __host__ __device__ inline int dimof(const DevBlock &b, int d) { return d == 0 ? b.ni : (d == 1 ? b.nj : b.nk); }
 
 // stride (in elements) along direction d
