@@ -171,12 +171,14 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
     }
     __syncthreads();
     constexpr bool posmajor = (dir == 0);
+    const FastDiv dNL = fast_div_init(NL), d5NL = fast_div_init(5 * NL), dW = fast_div_init(W);
     // ---- stage the prim line (l = -2..n+3) and the metrics of this
     // direction (l = 1..n): one thread per (line, point), coalesced along the
     // line for i-lines and across the group's neighbouring lines otherwise
     for (int e = threadIdx.x; e < NL * W; e += blockDim.x) {
-        const int ln = posmajor ? e / W : e % NL;
-        const int p = posmajor ? e % W : e / NL;
+        const int qq = posmajor ? fdiv(e, dW) : fdiv(e, dNL);
+        const int ln = posmajor ? qq : e - qq * NL;
+        const int p = posmajor ? e - qq * W : qq;
         const InvLine &L = lines[ln];
         const long long gi = L.dqbase + (long long)(p - 2) * L.stride;
         double v[8];
@@ -207,7 +209,8 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
         const int NP = n + 2;
         const int nitems = NL * 5 * NP;
         for (int idx = threadIdx.x; idx < nitems; idx += blockDim.x) {
-            const int ln = idx % NL, m = (idx / NL) % 5, i = idx / (5 * NL);
+            const int q1 = fdiv(idx, dNL), i = fdiv(idx, d5NL);
+            const int ln = idx - q1 * NL, m = q1 - 5 * i;
             const InvLine &L = lines[ln];
             if (i < L.ist || i > L.ied + 1) continue;
             double *ql_ = smem + (size_t)ln * LS + work0;
@@ -246,8 +249,8 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
         const int NT = H + 26;
         int nbad = 0;
         for (int idx = threadIdx.x; idx < NL * NT; idx += blockDim.x) {
-            const int ln = idx % NL;
-            const int t = idx / NL;
+            const int t = fdiv(idx, dNL);
+            const int ln = idx - t * NL;
             const InvLine &L = lines[ln];
             const double *ql_ = smem + (size_t)ln * LS + work0;
             const double *qr_ = ql_ + (size_t)5 * H;
@@ -321,7 +324,8 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
     {
         const int nitems = NL * n * 5;
         for (int idx = threadIdx.x; idx < nitems; idx += blockDim.x) {
-            const int ln = idx % NL, m = (idx / NL) % 5, l = 1 + idx / (5 * NL);
+            const int q1 = fdiv(idx, dNL), l0 = fdiv(idx, d5NL);
+            const int ln = idx - q1 * NL, m = q1 - 5 * l0, l = 1 + l0;
             const InvLine &L = lines[ln];
             const double *f_ = smem + (size_t)ln * LS + work0 + (size_t)10 * H;
             const double *sc = smem + (size_t)ln * LS + work0 + (size_t)15 * H;

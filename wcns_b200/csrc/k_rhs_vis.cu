@@ -126,14 +126,16 @@ __global__ void __launch_bounds__(256, 3) k_rhs_vis(DevParams P, DevFields F, co
     }
     __syncthreads();
     const bool posmajor = (dir == 0);
+    const FastDiv dNL = fast_div_init(NL), dW = fast_div_init(W);
     // ---- stage the line inputs: one thread per (line, point), all VIS_NF
     // loads of the point issued back to back (coalesced along the line for
     // i-lines, across the group's neighbouring lines otherwise)
     {
         const int g0 = dir == 0 ? 1 : 0, g1 = dir == 2 ? 1 : 2;  // the two other directions
         for (int e = threadIdx.x; e < NL * W; e += blockDim.x) {
-            const int ln = posmajor ? e / W : e % NL;
-            const int p = posmajor ? e % W : e / NL;
+            const int qq = posmajor ? fdiv(e, dW) : fdiv(e, dNL);
+            const int ln = posmajor ? qq : e - qq * NL;
+            const int p = posmajor ? e - qq * W : qq;
             const VisLine &L = lines[ln];
             const int l = p - 1;
             const long long gi = L.l0 + (long long)l * L.st;
@@ -164,8 +166,8 @@ __global__ void __launch_bounds__(256, 3) k_rhs_vis(DevParams P, DevFields F, co
     // ---- per half node: viscous flux fv (line-fastest in every direction, so
     // that the lanes of a warp share a position and its control path)
     for (int idx = threadIdx.x; idx < NL * H; idx += blockDim.x) {
-        const int ln = idx % NL;
-        const int h = idx / NL;
+        const int h = fdiv(idx, dNL);
+        const int ln = idx - h * NL;
         const VisLine &L = lines[ln];
         const double *S = smem + (size_t)ln * LS;
         auto at = [&](int f, int x) { return S[f * W + x + 1]; };
@@ -263,8 +265,9 @@ __global__ void __launch_bounds__(256, 3) k_rhs_vis(DevParams P, DevFields F, co
     __syncthreads();
     // ---- per point: FLUX_DXYZ and dq -= re*dfv
     for (int idx = threadIdx.x; idx < NL * n; idx += blockDim.x) {
-        const int ln = idx % NL;
-        const int l = 1 + idx / NL;
+        const int l0 = fdiv(idx, dNL);
+        const int ln = idx - l0 * NL;
+        const int l = 1 + l0;
         const VisLine &L = lines[ln];
         const double *fv = smem + (size_t)ln * LS + (size_t)VIS_NF * W;
         long long gi = L.l0 + (long long)l * L.st;

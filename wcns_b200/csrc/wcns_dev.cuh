@@ -112,6 +112,21 @@ __host__ __device__ inline long long gidx(const DevBlock &b, int i, int j, int k
     return b.off + (long long)(i + 2) + (long long)b.gx * ((long long)(j + 2) + (long long)b.gy * (long long)(k + 2));
 }
 
+// Division by a divisor that is the same for the whole kernel: one high
+// multiply instead of a division sequence.  Exact for 0 <= n, d and
+// n * d < 2^32 (m = ceil(2^32 / d); the error n * (m - 2^32/d) / 2^32 < n / 2^32
+// stays below 1/d).
+struct FastDiv {
+    unsigned d, m;
+};
+__host__ __device__ inline FastDiv fast_div_init(int d) {
+    FastDiv f;
+    f.d = (unsigned)d;
+    f.m = d <= 1 ? 0u : 0xFFFFFFFFu / (unsigned)d + 1u;
+    return f;
+}
+__device__ __forceinline__ int fdiv(int n, FastDiv f) { return f.d <= 1 ? n : (int)__umulhi((unsigned)n, f.m); }
+
 // interior point index p = (i-1) + ni*((j-1) + nj*(k-1)) -> (i, j, k); 32-bit
 // divisions whenever p fits (every realistic block)
 __device__ __forceinline__ void decode_point(const DevBlock &B, long long p, int &i, int &j, int &k) {
