@@ -422,8 +422,26 @@ static int build_tables(WcnsContext *c) {
     L.comp_first = c->up(comp_first);
     L.comp_n = c->up(comp_n);
     L.mem_slot = c->up(mem_slot);
-    L.mem_comp = c->up(mem_comp);
-    L.mem_idx = c->up(mem_idx);
+    // the members' writes grouped by the block that owns the point (the
+    // block's cluster writes them after its two-block pairs)
+    {
+        std::vector<int> wr_comp, blk_wr_first(nbk + 1, 0);
+        std::vector<long long> wr_idx;
+        for (int b = 0; b < nbk; b++) {
+            blk_wr_first[b] = (int)wr_idx.size();
+            const long long lo = c->blk[b].d.off, hi = lo + (long long)c->blk[b].d.gx * c->blk[b].d.gy * c->blk[b].d.gz;
+            for (size_t e = 0; e < mem_idx.size(); e++)
+                if (mem_idx[e] >= lo && mem_idx[e] < hi) {
+                    wr_comp.push_back(mem_comp[e]);
+                    wr_idx.push_back(mem_idx[e]);
+                }
+        }
+        blk_wr_first[nbk] = (int)wr_idx.size();
+        if (wr_idx.size() != mem_idx.size()) { set_err("internal: a multi-block point outside every block"); return WCNS_ERR_ARGUMENT; }
+        L.mem_comp = c->up(wr_comp);
+        L.mem_idx = c->up(wr_idx);
+        L.blk_mem_first = c->up(blk_wr_first);
+    }
     // line groups for the residual kernels
     size_t inv_smem = 0, vis_smem = 0;
     for (int dir = 0; dir < 3; dir++) {
@@ -848,15 +866,15 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
         launch_rhs_dirs(L, true);
         for (int d = 0; d < 3; d++) n += L.vis[d].ngroups ? 1 : 0;
         n += (L.vis[1].ngroups || L.vis[2].ngroups) ? 1 : 0;
-        launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
+        launch_communicate(L, 0); n += L.nsnap ? 2 : 0;
     }
     launch_rhs_dirs(L, false);
     for (int d = 0; d < 3; d++) n += L.inv[d].ngroups ? 1 : 0;
     n += (L.inv[1].ngroups || L.inv[2].ngroups) ? 1 : 0;
-    launch_communicate(L, 0); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
+    launch_communicate(L, 0); n += L.nsnap ? 2 : 0;
     launch_lhs(L); n += 6 + (L.nzero ? 2 : 0);  // prep, four sweeps, plane-major dq to the fields
     launch_update(L); n += 2;
-    launch_communicate(L, 1); n += L.nsnap ? (L.nmem ? 3 : 2) : 0;
+    launch_communicate(L, 1); n += L.nsnap ? 2 : 0;
     launch_residual(L, rms_slot); n += 2;
     c->launches = n;
     CK(cudaGetLastError());

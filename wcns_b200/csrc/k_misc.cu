@@ -241,7 +241,17 @@ __global__ void k_residual_partial(DevFields F, const DevBlock *__restrict__ blo
     long long np = (mi > 0 && mj > 0 && mk > 0) ? (long long)mi * mj * mk : 0;
     double s = 0.0, mx = 0.0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < np; q += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(q % mi) + 2, j = (int)((q / mi) % mj) + 2, k = (int)(q / ((long long)mi * mj)) + 2;
+        int i, j, k;
+        if (q < 0x7fffffffLL) {  // 32-bit divisions where they suffice
+            const int qq = (int)q, r = qq / mi;
+            i = qq - r * mi + 2;
+            j = r % mj + 2;
+            k = r / mj + 2;
+        } else {
+            i = (int)(q % mi) + 2;
+            j = (int)((q / mi) % mj) + 2;
+            k = (int)(q / ((long long)mi * mj)) + 2;
+        }
         long long id = gidx(B, i, j, k);
         double dtime1 = 1.0 / (F.f[F_DTDT][id] * F.f[F_VOL][id]);
 #pragma unroll
@@ -374,9 +384,16 @@ __global__ void k_snapshot(DevFields F, const long long *__restrict__ pts, int n
 // boundary_match_dq_2pm / boundary_match_pv_2pm: one cluster per block walks
 // the block's groups of independent pairs in order, with a cluster barrier
 // between groups (an edge point can belong to two regions; the host puts a
-// pair after every earlier pair it depends on).
-__global__ void k_match_2pm(DevFields F, const PairEntry *__restrict__ pairs, const int *__restrict__ blk_reg_first,
-                            const int *__restrict__ reg_pair_first, const double *__restrict__ snap, int nsnap, int which) {
+// pair after every earlier pair it depends on).  Then, as
+// boundary_match_dq_3pp / boundary_match_pv_3pp, the block's points shared
+// by more than two blocks take the mean over all copies (snapshot values,
+// member order); those means only read the snapshot and overwrite whatever
+// the pairs left at the point.
+__global__ void k_match(DevFields F, const PairEntry *__restrict__ pairs, const int *__restrict__ blk_reg_first,
+                        const int *__restrict__ reg_pair_first, const int *__restrict__ comp_first,
+                        const int *__restrict__ comp_n, const int *__restrict__ mem_slot,
+                        const int *__restrict__ mem_comp, const long long *__restrict__ mem_idx,
+                        const int *__restrict__ blk_mem_first, const double *__restrict__ snap, int nsnap, int which) {
     cg::cluster_group cluster = cg::this_cluster();
     const int bi = blockIdx.x / BC_CLUSTER;
     const int t0 = (int)cluster.block_rank() * blockDim.x + threadIdx.x, tstride = BC_CLUSTER * blockDim.x;
@@ -410,36 +427,16 @@ __global__ void k_match_2pm(DevFields F, const PairEntry *__restrict__ pairs, co
         }
         cluster.sync();
     }
-}
-
-// boundary_match_dq_3pp / boundary_match_pv_3pp: points shared by more than
-// two blocks take the mean over all copies (snapshot values, member order).
-// One thread per (field, member copy): the member slots are loaded ahead of
-// the values so that a thread waits on two dependent loads, not on 2*np.
-__global__ void k_match_3pp(DevFields F, const int *__restrict__ comp_first, const int *__restrict__ comp_n,
-                            const int *__restrict__ mem_slot, const int *__restrict__ mem_comp,
-                            const long long *__restrict__ mem_idx, int nmem, const double *__restrict__ snap,
-                            int nsnap, int which) {
     const int nf = which == 0 ? 5 : 6;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf * nmem; t += gridDim.x * blockDim.x) {
-        const int m = t / nmem, e = t - m * nmem;
-        const int c = mem_comp[e];
-        const int f0 = comp_first[c], np = comp_n[c];
+    const int e0 = blk_mem_first[bi], ne = blk_mem_first[bi + 1] - e0;
+    for (int t = t0; t < nf * ne; t += tstride) {
+        const int m = t / ne, e = e0 + (t - m * ne);
+        const int cc = mem_comp[e];
+        const int f0 = comp_first[cc], np = comp_n[cc];
         const long long id = mem_idx[e];
         const double *sm = snap + (long long)m * nsnap;
         double s = 0.0;
-        int q = 0;
-        for (; q + 4 <= np; q += 4) {
-            const int s0 = mem_slot[f0 + q], s1 = mem_slot[f0 + q + 1];
-            const int s2 = mem_slot[f0 + q + 2], s3 = mem_slot[f0 + q + 3];
-            double v0 = sm[s0], v1 = sm[s1], v2 = sm[s2], v3 = sm[s3];
-            if (which == 1) { v0 = v0 / 1.0; v1 = v1 / 1.0; v2 = v2 / 1.0; v3 = v3 / 1.0; }
-            s = s + v0;
-            s = s + v1;
-            s = s + v2;
-            s = s + v3;
-        }
-        for (; q < np; q++) {
+        for (int q = 0; q < np; q++) {
             double v = sm[mem_slot[f0 + q]];
             if (which == 1) v = v / 1.0;
             s = s + v;
@@ -453,12 +450,11 @@ __global__ void k_match_3pp(DevFields F, const int *__restrict__ comp_first, con
 void launch_communicate(const LaunchCtx &c, int which) {
     if (c.nsnap == 0) return;
     k_snapshot<<<(c.nsnap + 255) / 256, 256, 0, c.stream>>>(*c.F, c.snap_pts, c.nsnap, c.snap, which);
-    launch_block_clusters(k_match_2pm, c.nblocks, 256, c.stream, *c.F, (const PairEntry *)c.pairs,
-                          (const int *)c.blk_reg_first, (const int *)c.reg_pair_first, (const double *)c.snap, c.nsnap,
+    launch_block_clusters(k_match, c.nblocks, 256, c.stream, *c.F, (const PairEntry *)c.pairs,
+                          (const int *)c.blk_reg_first, (const int *)c.reg_pair_first, (const int *)c.comp_first,
+                          (const int *)c.comp_n, (const int *)c.mem_slot, (const int *)c.mem_comp,
+                          (const long long *)c.mem_idx, (const int *)c.blk_mem_first, (const double *)c.snap, c.nsnap,
                           which);
-    if (c.nmem > 0)
-        k_match_3pp<<<((which == 0 ? 5 : 6) * c.nmem + 127) / 128, 128, 0, c.stream>>>(*c.F, c.comp_first, c.comp_n, c.mem_slot, c.mem_comp,
-                                                             c.mem_idx, c.nmem, c.snap, c.nsnap, which);
 }
 
 }  // namespace wcns

@@ -81,8 +81,9 @@ struct LaunchCtx {
     int max_pair_regions = 0;
     int ncomp = 0, nmem = 0;
     int *comp_first = nullptr, *comp_n = nullptr, *mem_slot = nullptr;
-    int *mem_comp = nullptr;
-    long long *mem_idx = nullptr;
+    int *mem_comp = nullptr;        // members' writes grouped by block: component of the point
+    long long *mem_idx = nullptr;   // ... and the point (field index)
+    int *blk_mem_first = nullptr;   // per block (nblocks+1), first of its writes
     // residual
     double *res_partial = nullptr;  // per CTA partial sums
     int res_ctas_per_block = 0;
