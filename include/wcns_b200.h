@@ -71,6 +71,13 @@ int wcns_get_field(WcnsContext *ctx, int field, int nb, double *out);
  * what the flow-file write reads per block (write_flow_file_parallel,
  * parallel.f90:4073-4145). */
 int wcns_get_prim(WcnsContext *ctx, int nb, double *r, double *u, double *v, double *w, double *p, double *t);
+/* All blocks of the context at once, one synchronisation per call: the
+ * per-block loops of the set-up (init_nstart0/1 with recast_field,
+ * Sub2.f90:367-405) and of the flow-file write (parallel.f90:4073-4145).
+ * prim holds 6 pointers per block in block order: r, u, v, w, p, t (for
+ * wcns_get_prim_all a null t skips T of that block). */
+int wcns_set_prim_all(WcnsContext *ctx, const double *const *prim);
+int wcns_get_prim_all(WcnsContext *ctx, double *const *prim);
 int wcns_set_field(WcnsContext *ctx, int field, int nb, const double *in);
 
 /* Per-step drop-ins, in the reference's call order (Main.f90:85-109). */

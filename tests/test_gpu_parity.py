@@ -152,3 +152,24 @@ def test_get_prim_equals_get_field():
         g.get_prim(nb, out=five)
         for a, b in zip(five, got[:5]):
             assert np.array_equal(a, b)
+
+
+def test_all_block_state_transfer():
+    """wcns_set_prim_all / wcns_get_prim_all move every block's state with one
+    synchronisation and agree exactly with the per-block calls."""
+    case = cases.small_plate_case()
+    from wcns_b200.solver import Wcns
+    a, b = Wcns(case), Wcns(case)
+    a.step(2)
+    states = [a.get_prim(nb) for nb in range(1, case.nblocks + 1)]
+    b.set_prim_all(states)
+    outs = [[np.zeros_like(x) for x in st[:5]] for st in states]
+    b.get_prim_all(outs)
+    for st, out in zip(states, outs):
+        for x, y in zip(st[:5], out):
+            assert np.array_equal(x, y)
+    a.step(3)
+    b.step(3)
+    for nb in range(1, case.nblocks + 1):
+        for x, y in zip(a.get_prim(nb), b.get_prim(nb)):
+            assert np.array_equal(x, y)

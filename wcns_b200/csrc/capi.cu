@@ -783,6 +783,59 @@ extern "C" int wcns_get_prim(WcnsContext *c, int nb, double *r, double *u, doubl
     return 0;
 }
 
+// All blocks at once: the copies of every block go into the stream and the
+// call synchronises once (the per-block loop of the reference's set-up and
+// flow-file write).  prim: 6 pointers per block, r u v w p t.
+extern "C" int wcns_set_prim_all(WcnsContext *c, const double *const *prim) {
+    if (!c || !prim) { set_err("wcns_set_prim_all: null argument"); return WCNS_ERR_ARGUMENT; }
+    const int nbk = (int)c->blk.size();
+    for (int e = 0; e < 6 * nbk; e++)
+        if (!prim[e]) { set_err("wcns_set_prim_all: null array"); return WCNS_ERR_ARGUMENT; }
+    // the copies are spread over the context's three streams so that their
+    // set-up overlaps, after the work already queued on the context's stream;
+    // the call returns once all have landed
+    CK(cudaEventRecord(c->L.ev_fork, c->stream));
+    cudaStream_t st[3] = {c->stream, c->L.side[0], c->L.side[1]};
+    for (int q = 1; q < 3; q++) CK(cudaStreamWaitEvent(st[q], c->L.ev_fork, 0));
+    int e = 0;
+    for (int b = 0; b < nbk; b++) {
+        const DevBlock &d = c->blk[b].d;
+        const size_t n = (size_t)d.gx * d.gy * d.gz;
+        for (int f = 0; f < 6; f++, e++)
+            CK(cudaMemcpyAsync(c->F.f[F_R + f] + d.off, prim[6 * b + f], sizeof(double) * n, cudaMemcpyHostToDevice,
+                               st[e % 3]));
+    }
+    for (int q = 0; q < 3; q++) CK(cudaStreamSynchronize(st[q]));
+    return 0;
+}
+
+// prim: 6 pointers per block, r u v w p t; a null t skips T of that block.
+extern "C" int wcns_get_prim_all(WcnsContext *c, double *const *prim) {
+    if (!c || !prim) { set_err("wcns_get_prim_all: null argument"); return WCNS_ERR_ARGUMENT; }
+    const int nbk = (int)c->blk.size();
+    for (int b = 0; b < nbk; b++)
+        for (int f = 0; f < 5; f++)
+            if (!prim[6 * b + f]) { set_err("wcns_get_prim_all: null array"); return WCNS_ERR_ARGUMENT; }
+    // the state is final once the work queued on the context's stream is
+    // done; the copies then spread over the three streams as above
+    CK(cudaEventRecord(c->L.ev_fork, c->stream));
+    cudaStream_t st[3] = {c->stream, c->L.side[0], c->L.side[1]};
+    for (int q = 1; q < 3; q++) CK(cudaStreamWaitEvent(st[q], c->L.ev_fork, 0));
+    int e = 0;
+    for (int b = 0; b < nbk; b++) {
+        const DevBlock &d = c->blk[b].d;
+        const size_t n = (size_t)d.gx * d.gy * d.gz;
+        for (int f = 0; f < 6; f++)
+            if (prim[6 * b + f]) {
+                CK(cudaMemcpyAsync(prim[6 * b + f], c->F.f[F_R + f] + d.off, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                   st[e % 3]));
+                e++;
+            }
+    }
+    for (int q = 0; q < 3; q++) CK(cudaStreamSynchronize(st[q]));
+    return 0;
+}
+
 extern "C" int wcns_set_field(WcnsContext *c, int field, int nb, const double *in) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;

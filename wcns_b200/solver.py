@@ -103,6 +103,43 @@ class Wcns:
         _check(_lib.load().wcns_get_prim(self.h, nb, *ptrs))
         return out
 
+    def set_prim_all(self, prims):
+        """Set r, u, v, w, p, T of every block (prims[nb-1] = six arrays) with
+        one synchronisation.  The arrays must be C-contiguous float64 in the
+        ghosted layout; they are used in place."""
+        if len(prims) != len(self.dims):
+            raise ValueError("one list of six arrays per block")
+        ptrs = []
+        for nb, arrs in enumerate(prims, start=1):
+            ptrs += self._checked(nb, arrs, 6)
+        vec = (C.c_void_p * len(ptrs))(*ptrs)
+        _check(_lib.load().wcns_set_prim_all(self.h, vec))
+
+    def get_prim_all(self, outs):
+        """Copy r, u, v, w, p (and T where a block's list has six arrays) of
+        every block into `outs` (outs[nb-1] = five or six arrays) with one
+        synchronisation."""
+        if len(outs) != len(self.dims):
+            raise ValueError("one list of five or six arrays per block")
+        ptrs = []
+        for nb, arrs in enumerate(outs, start=1):
+            if len(arrs) not in (5, 6):
+                raise ValueError("five or six arrays per block")
+            ptrs += self._checked(nb, arrs, len(arrs)) + ([None] if len(arrs) == 5 else [])
+        vec = (C.c_void_p * len(ptrs))(*ptrs)
+        _check(_lib.load().wcns_get_prim_all(self.h, vec))
+        return outs
+
+    def _checked(self, nb, arrs, n):
+        ni, nj, nk = self.dims[nb - 1]
+        shape = (nk + 6, nj + 6, ni + 6)
+        if len(arrs) != n:
+            raise ValueError(f"block {nb}: {n} arrays expected")
+        for a in arrs:
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(f"block {nb}: array has the wrong shape, dtype or layout")
+        return [a.ctypes.data for a in arrs]
+
     def set(self, name, nb, arr):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
         _check(_lib.load().wcns_set_field(self.h, FID[name], nb, arr.ctypes.data))
