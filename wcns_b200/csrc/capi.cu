@@ -456,8 +456,8 @@ static int build_tables(WcnsContext *c) {
                 int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
                 int na = dimof(D, a1), nb2 = dimof(D, a2);
                 size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : rhs_vis_line_bytes(n);
-                // at most 72 KB of staged lines per CTA: three 256-thread CTAs per SM
-                // (both kernels are bounded to 80 registers per thread for the same reason)
+                // at most 72 KB of staged lines per CTA: three 256-thread inviscid or two
+                // 384-thread viscous CTAs per SM (both kernels are bounded to 80 registers)
                 int NL = pass == 0 ? std::max(1, std::min({rhs_invis_max_lines(), 3072 / (5 * (n + 2)),
                                                            (int)((72 * 1024) / per_line)}))
                                    : std::max(1, std::min({rhs_vis_max_lines(), 512 / (n + 1), (int)((72 * 1024) / per_line)}));

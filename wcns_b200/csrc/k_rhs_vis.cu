@@ -86,6 +86,9 @@ struct VisLine {
 // vol; the two Sutherland viscosities.  Then the line's viscous flux, 5 x (n+1).
 constexpr int VIS_NF = 24;
 constexpr int VIS_MAX_LINES = 32;  // lines per CTA (short k-lines are grouped many to a CTA)
+// 384 threads: the half-node fluxes of two 129-point lines (260) in one pass;
+// two CTAs per SM at 80 registers
+constexpr int VIS_THREADS = 384;
 enum : int { VS_U = 0, VS_DN = 4, VS_MET = 12, VS_VOL = 21, VS_V1 = 22, VS_V2 = 23 };
 
 __host__ __device__ inline int vis_line_stride(int n) {
@@ -98,7 +101,7 @@ __host__ __device__ inline int vis_line_stride(int n) {
 // out == nullptr: dq -= re*dFv in place; otherwise re*dFv is stored in
 // out[m*stride + point] for an ordered combine (k_combine_dq)
 template <int dir>
-__global__ void __launch_bounds__(256, 3) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+__global__ void __launch_bounds__(VIS_THREADS, 2) k_rhs_vis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                     const LineGroup *__restrict__ groups, int hmax, double *out,
                                                     long long stride) {
     extern __shared__ double smem[];
@@ -293,9 +296,9 @@ void launch_rhs_vis(const LaunchCtx &c, int dir, cudaStream_t st, double *out) {
     const DirTable &T = c.vis[dir];
     if (T.ngroups == 0) return;
     const long long stride = c.total;
-    if (dir == 0) k_rhs_vis<0><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
-    else if (dir == 1) k_rhs_vis<1><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
-    else k_rhs_vis<2><<<T.ngroups, 256, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
+    if (dir == 0) k_rhs_vis<0><<<T.ngroups, VIS_THREADS, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
+    else if (dir == 1) k_rhs_vis<1><<<T.ngroups, VIS_THREADS, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
+    else k_rhs_vis<2><<<T.ngroups, VIS_THREADS, T.smem, st>>>(*c.P, *c.F, c.blocks, T.groups, T.hmax, out, stride);
 }
 
 void setup_rhs_vis_attrs(size_t max_smem) {
