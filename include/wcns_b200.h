@@ -35,7 +35,7 @@ typedef struct WcnsContext WcnsContext;
 typedef enum WcnsStatus {
     WCNS_OK = 0,
     WCNS_ERR_ARGUMENT = 1,   /* invalid input (replaces the reference's stop) */
-    WCNS_ERR_ROE = 2,        /* Roe flux c^2 <= 0 (flux.f90:179-182) */
+    WCNS_ERR_ROE = 2,        /* Roe flux c^2 <= 0 (flux.f90:179-182), Van Leer c^2 < 0 (flux.f90:432-436) */
     WCNS_ERR_UPDATE = 3,     /* too many non-physical points (Sub2.f90:781-785) */
     WCNS_ERR_CUDA = 4,
     WCNS_ERR_UNSUPPORTED = 5 /* BC type or field not handled (BC.f90:203-205) */

@@ -197,6 +197,63 @@ static void flux_sw(const Orc *o, const double *ql, const double *qr, double nx,
     for (int m = 0; m < 5; m++) f[m] = fl[m] + fr[m];
 }
 
+/* flux_vanleer_pn, flux.f90:410-501 (gethmgm -> gethmgm_ns,
+ * GasModel.f90:376-399): Van Leer's split flux of one state.  Returns
+ * nonzero when c^2 < 0 (the reference stops there).  (b +- 1)**2 is
+ * evaluated as a product, as gfortran does for an integer exponent 2. */
+static int flux_vl_pn(const Orc *o, const double *prim, double nx, double ny, double nz, double nt, double *f,
+                      int npn) {
+    double gama = o->gama;
+    double rm = prim[0], um = prim[1], vm = prim[2], wm = prim[3], pm = prim[4];
+    double u2 = 0.5 * (um * um + vm * vm + wm * wm);
+    double hint = gama / (gama - 1.0) * pm / rm;
+    double hm = hint + u2;
+    double c2 = gama * pm / rm;
+    int bad = c2 < 0.0;
+    double cm = sqrt(c2);
+    double ct = nx * um + ny * vm + nz * wm + nt;
+    double cgm = sqrt(nx * nx + ny * ny + nz * nz) + SML_SSS;
+    double cgm1 = 1.0 / cgm;
+    double nxa = nx * cgm1, nya = ny * cgm1, nza = nz * cgm1;
+    double cta = ct * cgm1;
+    double bmvl = cta / cm;
+    for (int m = 0; m < 5; m++) f[m] = 0.0;
+    if (fabs(bmvl) < 1.0) {
+        double ctcm, b;
+        if (npn == 1) {
+            ctcm = (-cta + 2.0 * cm) / gama;
+            b = (bmvl + 1.0) * (bmvl + 1.0);
+            f[0] = 0.25 * cgm * rm * cm * b;
+        } else {
+            ctcm = (-cta - 2.0 * cm) / gama;
+            b = (bmvl - 1.0) * (bmvl - 1.0);
+            f[0] = -(0.25 * cgm * rm * cm * b);
+        }
+        f[1] = f[0] * (um + nxa * ctcm);
+        f[2] = f[0] * (vm + nya * ctcm);
+        f[3] = f[0] * (wm + nza * ctcm);
+        f[4] = f[0] * hm;
+    } else if (npn == 1 ? bmvl >= 1.0 : bmvl <= -1.0) {
+        double rmct = rm * cta;
+        f[0] = cgm * rmct;
+        f[1] = cgm * (rmct * um + pm * nxa);
+        f[2] = cgm * (rmct * vm + pm * nya);
+        f[3] = cgm * (rmct * wm + pm * nza);
+        f[4] = cgm * rmct * hm;
+    }
+    return bad;
+}
+
+/* flux_vanleer, flux.f90:395-408 */
+static int flux_vanleer(const Orc *o, const double *ql, const double *qr, double nx, double ny, double nz, double nt,
+                        double *f) {
+    double fl[5], fr[5];
+    int bad = flux_vl_pn(o, ql, nx, ny, nz, nt, fl, 1);
+    bad += flux_vl_pn(o, qr, nx, ny, nz, nt, fr, -1);
+    for (int m = 0; m < 5; m++) f[m] = fl[m] + fr[m];
+    return bad;
+}
+
 /* flux, Convect.f90:1245-1272 with getem GasModel.f90:358-374 */
 static void phys_flux(double gama, const double *prim, double nx, double ny, double nz, double nt, double *f) {
     double rm = prim[0], um = prim[1], vm = prim[2], wm = prim[3], pm = prim[4];
@@ -270,11 +327,14 @@ static int flux_roe(const Orc *o, const double *qlin, const double *qrin, double
     return bad;
 }
 
+/* the flux routine chosen by nflux (Convect.f90:12-46): 1 Steger-Warming,
+ * 2 Van Leer, 3 Roe */
 static int flux_type(const Orc *o, const double *ql, const double *qr, const double *nx4, double *f) {
     if (o->prm.nflux == 1) {
         flux_sw(o, ql, qr, nx4[0], nx4[1], nx4[2], nx4[3], f, o->prm.efix);
         return 0;
     }
+    if (o->prm.nflux == 2) return flux_vanleer(o, ql, qr, nx4[0], nx4[1], nx4[2], nx4[3], f);
     return flux_roe(o, ql, qr, nx4[0], nx4[1], nx4[2], nx4[3], f, o->prm.efix);
 }
 

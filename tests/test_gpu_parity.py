@@ -39,6 +39,10 @@ CASES = {
     "plate_small_sym2d": lambda: cases.small_plate_case(nk=4),
     "supersonic_box_roe41": lambda: supersonic_box_case(),
     "supersonic_box_sw4": lambda: supersonic_box_case(nscheme=4, nflux=1),
+    # Van Leer flux (nflux 2): subsonic vortex and plate, supersonic box
+    "vortex_vl_4": lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=4, nflux=2),
+    "plate_small_vl41": lambda: cases.small_plate_case(nflux=2),
+    "supersonic_box_vl41": lambda: supersonic_box_case(nscheme=41, nflux=2),
 }
 
 

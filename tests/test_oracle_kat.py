@@ -93,7 +93,25 @@ def test_steger_warming_split_sums_to_flux(L, oracle_lib):
         np.testing.assert_allclose(f_sw, f_phys, rtol=1e-12, atol=1e-12 * np.abs(f_phys).max())
 
 
-@pytest.mark.parametrize("nscheme,nflux", [(4, 1), (41, 1), (4, 3), (41, 3)])
+def test_van_leer_split_sums_to_flux(L, oracle_lib):
+    """flux_vanleer of equal states: the positive and negative parts of Van
+    Leer's splitting add up to the physical flux, subsonic and supersonic."""
+    rng = np.random.default_rng(4)
+    prm = _prm(oracle_lib)
+    seen = set()
+    for _ in range(40):
+        q = np.ascontiguousarray([rng.uniform(0.5, 2.0), *rng.uniform(-2.5, 2.5, 3), rng.uniform(0.5, 4.0)])
+        n4 = np.ascontiguousarray([*rng.uniform(-1, 1, 3), 0.0])
+        mach = abs(q[1:4] @ n4[:3]) / np.linalg.norm(n4[:3]) / np.sqrt(1.4 * q[4] / q[0])
+        seen.add(mach >= 1.0)
+        f_phys, f_vl = np.zeros(5), np.zeros(5)
+        L.orc_fluxes(C.byref(prm), 0, _p(q), _p(q), _p(n4), _p(f_phys))
+        L.orc_fluxes(C.byref(prm), 2, _p(q), _p(q), _p(n4), _p(f_vl))
+        np.testing.assert_allclose(f_vl, f_phys, rtol=1e-12, atol=1e-12 * np.abs(f_phys).max())
+    assert seen == {True, False}
+
+
+@pytest.mark.parametrize("nscheme,nflux", [(4, 1), (41, 1), (4, 2), (41, 2), (4, 3), (41, 3)])
 def test_wcns_line_uniform_state_has_zero_residual(L, oracle_lib, nscheme, nflux):
     ni = 11
     p = cases.Params(moo=0.5, nscheme=nscheme, nflux=nflux)

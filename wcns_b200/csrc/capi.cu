@@ -512,7 +512,11 @@ static int check_errors(WcnsContext *c) {
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaMemcpy(h, c->d_err, sizeof h, cudaMemcpyDeviceToHost));
     CK(cudaMemset(c->d_err, 0, sizeof h));
-    if (h[ERR_ROE]) { set_err("flux_Roe: c^2 <= 0 at " + std::to_string(h[ERR_ROE]) + " half nodes"); return WCNS_ERR_ROE; }
+    if (h[ERR_ROE]) {
+        set_err(std::string(c->P.nflux == 2 ? "flux_vanleer: c^2 < 0" : "flux_Roe: c^2 <= 0") + " at " +
+                std::to_string(h[ERR_ROE]) + " half-node states");
+        return WCNS_ERR_ROE;
+    }
     if (h[ERR_UPDATE_BLOCKS]) { set_err("update_limited: too many non-physical points"); return WCNS_ERR_UPDATE; }
     if (h[ERR_TIMEOUT]) { set_err("LU-SGS sweep: a bounded wait for a plane's coefficients ran out"); return WCNS_ERR_CUDA; }
     return 0;
@@ -526,7 +530,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
         return WCNS_ERR_ARGUMENT;
     }
     if (prm->nscheme != 4 && prm->nscheme != 41) { set_err("nscheme must be 4 or 41"); return WCNS_ERR_UNSUPPORTED; }
-    if (prm->nflux != 1 && prm->nflux != 3) { set_err("nflux must be 1 (Steger-Warming) or 3 (Roe)"); return WCNS_ERR_UNSUPPORTED; }
+    if (prm->nflux < 1 || prm->nflux > 3) { set_err("nflux must be 1 (Steger-Warming), 2 (Van Leer) or 3 (Roe)"); return WCNS_ERR_UNSUPPORTED; }
     if (prm->nvis != 0 && prm->nvis != 1) { set_err("nvis must be 0 or 1"); return WCNS_ERR_ARGUMENT; }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { set_err("no CUDA device"); return WCNS_ERR_CUDA; }

@@ -238,6 +238,53 @@ __device__ __forceinline__ void flux_sw_pn(const DevParams &P, const double *pri
     f[4] = (l1 * em - x1 * hm + cta * x2) * rm;
 }
 
+// flux_vanleer_pn (flux.f90:410-501), gethmgm -> gethmgm_ns
+// (GasModel.f90:376-399).  Returns 1 when c^2 < 0 (the reference stops).
+// (b +- 1)**2 is a product, as gfortran evaluates an integer exponent 2.
+__device__ __forceinline__ int flux_vl_pn(const DevParams &P, const double *prim, double nx, double ny, double nz,
+                                          double nt, double *f, int npn) {
+    const double gama = P.gama;
+    double rm = prim[0], um = prim[1], vm = prim[2], wm = prim[3], pm = prim[4];
+    double u2 = 0.5 * (um * um + vm * vm + wm * wm);
+    double hint = P.g1 * pm / rm;
+    double hm = hint + u2;
+    double c2 = gama * pm / rm;
+    const int bad = c2 < 0.0 ? 1 : 0;
+    double cm = sqrt(c2);
+    double ct = nx * um + ny * vm + nz * wm + nt;
+    double cgm = sqrt(nx * nx + ny * ny + nz * nz) + SML_SSS;
+    double cgm1 = 1.0 / cgm;
+    double nxa = nx * cgm1, nya = ny * cgm1, nza = nz * cgm1;
+    double cta = ct * cgm1;
+    double bmvl = cta / cm;
+#pragma unroll
+    for (int m = 0; m < 5; m++) f[m] = 0.0;
+    if (fabs(bmvl) < 1.0) {
+        double ctcm, b;
+        if (npn == 1) {
+            ctcm = (-cta + 2.0 * cm) / gama;
+            b = (bmvl + 1.0) * (bmvl + 1.0);
+            f[0] = 0.25 * cgm * rm * cm * b;
+        } else {
+            ctcm = (-cta - 2.0 * cm) / gama;
+            b = (bmvl - 1.0) * (bmvl - 1.0);
+            f[0] = -(0.25 * cgm * rm * cm * b);
+        }
+        f[1] = f[0] * (um + nxa * ctcm);
+        f[2] = f[0] * (vm + nya * ctcm);
+        f[3] = f[0] * (wm + nza * ctcm);
+        f[4] = f[0] * hm;
+    } else if (npn == 1 ? bmvl >= 1.0 : bmvl <= -1.0) {
+        double rmct = rm * cta;
+        f[0] = cgm * rmct;
+        f[1] = cgm * (rmct * um + pm * nxa);
+        f[2] = cgm * (rmct * vm + pm * nya);
+        f[3] = cgm * (rmct * wm + pm * nza);
+        f[4] = cgm * rmct * hm;
+    }
+    return bad;
+}
+
 // flux (Convect.f90:1245-1272) with getem (GasModel.f90:358-374)
 __device__ __forceinline__ void phys_flux(double gama, const double *prim, double nx, double ny, double nz, double nt,
                                           double *f) {
@@ -317,8 +364,18 @@ __device__ __forceinline__ int flux_roe(const DevParams &P, const double *qlin, 
     return bad;
 }
 
+// the flux routine chosen by nflux (Convect.f90:12-46): 1 Steger-Warming,
+// 2 Van Leer, 3 Roe.  Returns the number of c^2 failures.
 __device__ __forceinline__ int flux_type(const DevParams &P, const double *ql, const double *qr, double nx, double ny,
                                          double nz, double nt, double *f) {
+    if (P.nflux == 2) {
+        double fl[5], fr[5];
+        int bad = flux_vl_pn(P, ql, nx, ny, nz, nt, fl, 1);
+        bad += flux_vl_pn(P, qr, nx, ny, nz, nt, fr, -1);
+#pragma unroll
+        for (int m = 0; m < 5; m++) f[m] = fl[m] + fr[m];
+        return bad;
+    }
     if (P.nflux == 1) {
         double fl[5], fr[5];
         flux_sw_pn(P, ql, nx, ny, nz, nt, fl, 1);
