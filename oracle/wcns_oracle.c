@@ -339,8 +339,11 @@ static int flux_type(const Orc *o, const double *ql, const double *qr, const dou
 }
 
 /* ------------------------------------------------------------------ */
-/* WCNS-E-5 line scheme: WCNS_E_5 (WCNSE5.f90:2-206, nscheme=4) and     */
-/* WCNS_E_5_41 (WCNSE5.f90:2087-2759, nscheme=41).                     */
+/* WCNS-E-5 line scheme: WCNS_E_5 (WCNSE5.f90:2-206, nscheme=4),       */
+/* WCNS_E_5_41 (WCNSE5.f90:2087-2759, nscheme=41) and WCNS_E_5_42       */
+/* (WCNSE5.f90:2766-3438, nscheme=42: the same boundary sections with   */
+/* second-order states at the first four half nodes of each end,        */
+/* WCNSE5.f90:2967-2986 and 3207-3226).                                 */
 /* q: prim line, q[m*L + (i+2)], i=-2..n+3, L=n+6.                      */
 /* nx: half-node metrics nx[c + 4*i], i=0..n.                           */
 /* df: df[m + 5*(i-1)], i=1..n.  Returns count of Roe c^2<=0 events.    */
@@ -437,7 +440,8 @@ static int wcns_line(const Orc *o, int ni, const double *q, const double *nx, do
     }
     flux_dxyz(5, ni, f, df);
 
-    if (o->prm.nscheme == 41) {
+    if (o->prm.nscheme == 41 || o->prm.nscheme == 42) {
+        const int s42 = o->prm.nscheme == 42;
         double u_l_old[5][9], u_r_old[5][9];
         if (ist > 1) {
             for (int i = 1; i <= 4; i++)
@@ -447,13 +451,20 @@ static int wcns_line(const Orc *o, int ni, const double *q, const double *nx, do
                 }
             /* (1) boundary point 1 */
             for (int m = 0; m < 5; m++) {
-                QWL(m, 0) = (3.0 * QL(m, 1) - 1.0 * QL(m, 2) - 0. * QL(m, 3)) / 2.0;
+                if (s42) {
+                    QWL(m, 0) = (677.0 * QL(m, 1) - 421.0 * QL(m, 2) + 99.0 * QL(m, 3) + 13.0 * QL(m, 4)) / 368.0;
+                    QWL(m, 1) = (5.0 * QL(m, 1) + 15.0 * QL(m, 2) - 5.0 * QL(m, 3) + QL(m, 4)) / 16.0;
+                    QWL(m, 2) = (-QL(m, 1) + 9.0 * QL(m, 2) + 9.0 * QL(m, 3) - QL(m, 4)) / 16.0;
+                    QWL(m, 3) = (QL(m, 1) - 5.0 * QL(m, 2) + 15.0 * QL(m, 3) + 5.0 * QL(m, 4)) / 16.0;
+                } else {
+                    QWL(m, 0) = (3.0 * QL(m, 1) - 1.0 * QL(m, 2) - 0. * QL(m, 3)) / 2.0;
+                    QWL(m, 1) = (19.0 * QL(m, 1) + 25.0 * QL(m, 2) - 2. * QL(m, 3)) / 42.0;
+                    QWL(m, 2) = (4.0 * QL(m, 1) + 3.0 * QL(m, 2) + 9.0 * QL(m, 3) + 2. * QL(m, 4)) / 18.0;
+                    QWL(m, 3) = (-2.0 * QL(m, 1) + 3.0 * QL(m, 2) + 3.0 * QL(m, 3) + 2. * QL(m, 4)) / 6.0;
+                }
                 QWR(m, 0) = QWL(m, 0);
-                QWL(m, 1) = (19.0 * QL(m, 1) + 25.0 * QL(m, 2) - 2. * QL(m, 3)) / 42.0;
                 QWR(m, 1) = QWL(m, 1);
-                QWL(m, 2) = (4.0 * QL(m, 1) + 3.0 * QL(m, 2) + 9.0 * QL(m, 3) + 2. * QL(m, 4)) / 18.0;
                 QWR(m, 2) = QWL(m, 2);
-                QWL(m, 3) = (-2.0 * QL(m, 1) + 3.0 * QL(m, 2) + 3.0 * QL(m, 3) + 2. * QL(m, 4)) / 6.0;
                 QWR(m, 3) = QWL(m, 3);
             }
             for (int i = 0; i <= 3; i++) {
@@ -538,13 +549,20 @@ static int wcns_line(const Orc *o, int ni, const double *q, const double *nx, do
             }
             /* (4) boundary point N */
             for (int m = 0; m < 5; m++) {
-                QWR(m, ni) = (3.0 * QL(m, ni) - 1.0 * QL(m, ni - 1) - 0. * QL(m, ni - 2)) / 2.0;
+                if (s42) {
+                    QWR(m, ni) = (677.0 * QL(m, ni) - 421.0 * QL(m, ni - 1) + 99.0 * QL(m, ni - 2) + 13.0 * QL(m, ni - 3)) / 368.0;
+                    QWR(m, ni - 1) = (5.0 * QL(m, ni) + 15.0 * QL(m, ni - 1) - 5.0 * QL(m, ni - 2) + QL(m, ni - 3)) / 16.0;
+                    QWR(m, ni - 2) = (-QL(m, ni) + 9.0 * QL(m, ni - 1) + 9.0 * QL(m, ni - 2) - QL(m, ni - 3)) / 16.0;
+                    QWR(m, ni - 3) = (QL(m, ni) - 5.0 * QL(m, ni - 1) + 15.0 * QL(m, ni - 2) + 5.0 * QL(m, ni - 3)) / 16.0;
+                } else {
+                    QWR(m, ni) = (3.0 * QL(m, ni) - 1.0 * QL(m, ni - 1) - 0. * QL(m, ni - 2)) / 2.0;
+                    QWR(m, ni - 1) = (19.0 * QL(m, ni) + 25.0 * QL(m, ni - 1) - 2. * QL(m, ni - 2)) / 42.0;
+                    QWR(m, ni - 2) = (4.0 * QL(m, ni) + 3.0 * QL(m, ni - 1) + 9.0 * QL(m, ni - 2) + 2. * QL(m, ni - 3)) / 18.0;
+                    QWR(m, ni - 3) = (-2.0 * QL(m, ni) + 3.0 * QL(m, ni - 1) + 3.0 * QL(m, ni - 2) + 2. * QL(m, ni - 3)) / 6.0;
+                }
                 QWL(m, ni) = QWR(m, ni);
-                QWR(m, ni - 1) = (19.0 * QL(m, ni) + 25.0 * QL(m, ni - 1) - 2. * QL(m, ni - 2)) / 42.0;
                 QWL(m, ni - 1) = QWR(m, ni - 1);
-                QWR(m, ni - 2) = (4.0 * QL(m, ni) + 3.0 * QL(m, ni - 1) + 9.0 * QL(m, ni - 2) + 2. * QL(m, ni - 3)) / 18.0;
                 QWL(m, ni - 2) = QWR(m, ni - 2);
-                QWR(m, ni - 3) = (-2.0 * QL(m, ni) + 3.0 * QL(m, ni - 1) + 3.0 * QL(m, ni - 2) + 2. * QL(m, ni - 3)) / 6.0;
                 QWL(m, ni - 3) = QWR(m, ni - 3);
             }
             for (int i = ni; i >= ni - 3; i--) {

@@ -76,7 +76,7 @@ def test_create_rejects_unsupported_scheme_before_device_work():
     from wcns_b200.solver import params_struct
     lib = _lib.load()
     case = cases.small_plate_case()
-    case.params.nscheme = 42
+    case.params.nscheme = 45
     prm = params_struct(case.params)
     dims = (C.c_int * 3)(*case.dims[0])
     keep = [np.ascontiguousarray(a) for a in case.xyz[0]]

@@ -43,6 +43,10 @@ CASES = {
     "vortex_vl_4": lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=4, nflux=2),
     "plate_small_vl41": lambda: cases.small_plate_case(nflux=2),
     "supersonic_box_vl41": lambda: supersonic_box_case(nscheme=41, nflux=2),
+    # nscheme 42: the 41 boundary sections with second-order end states
+    "vortex_roe_42": lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=42, nflux=3),
+    "plate_small_roe42": lambda: cases.small_plate_case(nscheme=42),
+    "supersonic_box_sw42": lambda: supersonic_box_case(nscheme=42, nflux=1),
 }
 
 

@@ -111,7 +111,7 @@ def test_van_leer_split_sums_to_flux(L, oracle_lib):
     assert seen == {True, False}
 
 
-@pytest.mark.parametrize("nscheme,nflux", [(4, 1), (41, 1), (4, 2), (41, 2), (4, 3), (41, 3)])
+@pytest.mark.parametrize("nscheme,nflux", [(4, 1), (41, 1), (42, 1), (4, 2), (41, 2), (42, 2), (4, 3), (41, 3), (42, 3)])
 def test_wcns_line_uniform_state_has_zero_residual(L, oracle_lib, nscheme, nflux):
     ni = 11
     p = cases.Params(moo=0.5, nscheme=nscheme, nflux=nflux)
@@ -122,6 +122,27 @@ def test_wcns_line_uniform_state_has_zero_residual(L, oracle_lib, nscheme, nflux
     df = np.zeros(5 * ni)
     assert L.orc_wcns_line(C.byref(prm), ni, _p(q), _p(nx), _p(df)) == 0
     assert np.abs(df).max() <= 1e-13
+
+
+@pytest.mark.parametrize("nscheme", [41, 42])
+@pytest.mark.parametrize("nflux", [1, 2, 3])
+def test_wcns_line_sections_keep_a_uniform_state(L, oracle_lib, nscheme, nflux):
+    """With both line ends flagged as physical boundaries (third ghost layer
+    density negative, as the wall and far-field conditions leave it), the
+    boundary sections of nscheme 41 and 42 run; their end states reproduce
+    a constant, so a uniform state still has a zero residual."""
+    ni = 13
+    p = cases.Params(moo=0.5, nscheme=nscheme, nflux=nflux)
+    prm = oracle_lib.params_struct(p)
+    roo, uoo, voo, woo, poo = p.freestream()
+    q = np.repeat([roo, uoo, voo, woo, poo], ni + 6).reshape(5, ni + 6)
+    q[0, 0] = -roo
+    q[0, ni + 5] = -roo
+    q = np.ascontiguousarray(q)
+    nx = np.ascontiguousarray(np.tile([0.7, 0.2, -0.1, 0.0], ni + 1))
+    df = np.zeros(5 * ni)
+    assert L.orc_wcns_line(C.byref(prm), ni, _p(q), _p(nx), _p(df)) == 0
+    assert np.abs(df).max() <= 1e-12
 
 
 def wavy_freestream_case(nvis, nscheme=41, nflux=3, dims=(17, 13, 9)):

@@ -529,7 +529,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
         set_err("wcns_create: invalid argument");
         return WCNS_ERR_ARGUMENT;
     }
-    if (prm->nscheme != 4 && prm->nscheme != 41) { set_err("nscheme must be 4 or 41"); return WCNS_ERR_UNSUPPORTED; }
+    if (prm->nscheme != 4 && prm->nscheme != 41 && prm->nscheme != 42) { set_err("nscheme must be 4, 41 or 42"); return WCNS_ERR_UNSUPPORTED; }
     if (prm->nflux < 1 || prm->nflux > 3) { set_err("nflux must be 1 (Steger-Warming), 2 (Van Leer) or 3 (Roe)"); return WCNS_ERR_UNSUPPORTED; }
     if (prm->nvis != 0 && prm->nvis != 1) { set_err("nvis must be 0 or 1"); return WCNS_ERR_ARGUMENT; }
     int dev = 0;

@@ -2,16 +2,18 @@
 //
 // Restates r_h_s_invis (RHS.f90:35-72) -> invcode -> inviscd3d
 // (Convect.f90:2-56, 58-649) with the WCNS-E-5 line scheme WCNS_E_5
-// (WCNSE5.f90:2-206, nscheme=4) or WCNS_E_5_41 (WCNSE5.f90:2087-2759,
-// nscheme=41), Steger-Warming (flux.f90:2-77) or Roe (flux.f90:116-244)
-// fluxes, and FLUX_DXYZ (WCNSE5.f90:209-254).  dq += dF.
+// (WCNSE5.f90:2-206, nscheme=4), WCNS_E_5_41 (WCNSE5.f90:2087-2759,
+// nscheme=41) or WCNS_E_5_42 (WCNSE5.f90:2766-3438, nscheme=42, the 41
+// sections with second-order end states), Steger-Warming (flux.f90:2-77),
+// Van Leer (flux.f90:395-501) or Roe (flux.f90:116-244) fluxes, and
+// FLUX_DXYZ (WCNSE5.f90:209-254).  dq += dF.
 //
 // One CTA owns a group of NL lines of one block.  The reference's
 // sequential line loop is split into three parallel phases:
 //   A  per point i: smoothness indicators and nonlinear weights, giving the
 //      left state at half node i and the right state at half node i-1;
 //   B  per half node: boundary closures, positivity fallback, numerical flux;
-//      plus the 26 independent fluxes of the nscheme=41 boundary sections;
+//      plus the 26 independent fluxes of the nscheme=41/42 boundary sections;
 //   C  per point: sixth-order flux difference (or the boundary-section
 //      difference where the reference overrides it) accumulated into dq.
 // Each value is produced with the reference's exact operation sequence.
@@ -68,8 +70,15 @@ __device__ __forceinline__ double qwr_postB(const InvLine &L, const double *sqwr
     return sqwr[m * (n + 1) + h];
 }
 
-// Left boundary-section states (WCNSE5.f90:2284-2459)
-__device__ __forceinline__ double s1_state(const InvLine &L, int m, int h) {
+// Left boundary-section states (WCNSE5.f90:2284-2459); nscheme=42 has
+// second-order states at the first four half nodes (WCNSE5.f90:2967-2986)
+__device__ __forceinline__ double s1_state(const InvLine &L, int m, int h, bool s42) {
+    if (s42) switch (h) {
+        case 0: return (677.0 * qv(L, m, 1) - 421.0 * qv(L, m, 2) + 99.0 * qv(L, m, 3) + 13.0 * qv(L, m, 4)) / 368.0;
+        case 1: return (5.0 * qv(L, m, 1) + 15.0 * qv(L, m, 2) - 5.0 * qv(L, m, 3) + qv(L, m, 4)) / 16.0;
+        case 2: return (-qv(L, m, 1) + 9.0 * qv(L, m, 2) + 9.0 * qv(L, m, 3) - qv(L, m, 4)) / 16.0;
+        default: return (qv(L, m, 1) - 5.0 * qv(L, m, 2) + 15.0 * qv(L, m, 3) + 5.0 * qv(L, m, 4)) / 16.0;
+        }
     switch (h) {
     case 0: return (3.0 * qv(L, m, 1) - 1.0 * qv(L, m, 2) - 0. * qv(L, m, 3)) / 2.0;
     case 1: return (19.0 * qv(L, m, 1) + 25.0 * qv(L, m, 2) - 2. * qv(L, m, 3)) / 42.0;
@@ -94,10 +103,17 @@ __device__ __forceinline__ double s3_left(const InvLine &L, int m, int h) {
     if (h == 2) return (-29.0 * qv(L, m, 1) + 170.0 * qv(L, m, 2) + 63.0 * qv(L, m, 3) + 12.0 * qv(L, m, 4)) / 216.0;
     return s2_left(L, m, h);
 }
-// Right boundary-section states (WCNSE5.f90:2524-2705); h counts down from n
-__device__ __forceinline__ double s4_state(const InvLine &L, int m, int h) {
+// Right boundary-section states (WCNSE5.f90:2524-2705); h counts down from
+// n; nscheme=42 as on the left (WCNSE5.f90:3207-3226)
+__device__ __forceinline__ double s4_state(const InvLine &L, int m, int h, bool s42) {
     int n = L.n;
     int o = n - h;
+    if (s42) switch (o) {
+        case 0: return (677.0 * qv(L, m, n) - 421.0 * qv(L, m, n - 1) + 99.0 * qv(L, m, n - 2) + 13.0 * qv(L, m, n - 3)) / 368.0;
+        case 1: return (5.0 * qv(L, m, n) + 15.0 * qv(L, m, n - 1) - 5.0 * qv(L, m, n - 2) + qv(L, m, n - 3)) / 16.0;
+        case 2: return (-qv(L, m, n) + 9.0 * qv(L, m, n - 1) + 9.0 * qv(L, m, n - 2) - qv(L, m, n - 3)) / 16.0;
+        default: return (qv(L, m, n) - 5.0 * qv(L, m, n - 1) + 15.0 * qv(L, m, n - 2) + 5.0 * qv(L, m, n - 3)) / 16.0;
+        }
     switch (o) {
     case 0: return (3.0 * qv(L, m, n) - 1.0 * qv(L, m, n - 1) - 0. * qv(L, m, n - 2)) / 2.0;
     case 1: return (19.0 * qv(L, m, n) + 25.0 * qv(L, m, n - 1) - 2. * qv(L, m, n - 2)) / 42.0;
@@ -128,8 +144,8 @@ __device__ __forceinline__ double s6_right(const InvLine &L, int m, int h) {
 // qwl(h) at the moment the right sections save u_l_old: the left sections'
 // final values where they ran (h<=5), otherwise the phase-B value.
 __device__ __forceinline__ double qwl_preright(const InvLine &L, const double *sqwl, int nscheme, int m, int h) {
-    if (nscheme == 41 && L.ist > 1 && h <= 5) {
-        if (h == 0) return s1_state(L, m, 0);
+    if ((nscheme == 41 || nscheme == 42) && L.ist > 1 && h <= 5) {
+        if (h == 0) return s1_state(L, m, 0, nscheme == 42);
         if (h == 2) return s3_left(L, m, 2);
         return s2_left(L, m, h);
     }
@@ -244,7 +260,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
         }
     }
     __syncthreads();
-    // ---- phase B: fluxes at half nodes, and the nscheme=41 boundary-section fluxes
+    // ---- phase B: fluxes at half nodes, and the nscheme=41/42 boundary-section fluxes
     {
         const int NT = H + 26;
         int nbad = 0;
@@ -262,7 +278,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
                 if (ql[0] <= RMIN_LIMIT || ql[4] <= PMIN_LIMIT) { int ii = h > 1 ? h : 1; for (int m = 0; m < 5; m++) ql[m] = qv(L, m, ii); }
                 if (qr[0] <= RMIN_LIMIT || qr[4] <= PMIN_LIMIT) { int ii = h + 1 < n ? h + 1 : n; for (int m = 0; m < 5; m++) qr[m] = qv(L, m, ii); }
             } else {
-                if (P.nscheme != 41) continue;
+                if (P.nscheme != 41 && P.nscheme != 42) continue;
                 int sidx = t - H;  // 0..25
                 if (sidx < 13) {
                     if (L.ist <= 1) continue;
@@ -278,10 +294,10 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
                 }
                 for (int m = 0; m < 5; m++) {
                     switch (mode) {
-                    case 1: ql[m] = qr[m] = s1_state(L, m, h); break;
+                    case 1: ql[m] = qr[m] = s1_state(L, m, h, P.nscheme == 42); break;
                     case 2: ql[m] = s2_left(L, m, h); qr[m] = s2_right(L, m, h); break;
                     case 3: ql[m] = s3_left(L, m, h); qr[m] = qwr_postB(L, qr_, m, h); break;
-                    case 4: ql[m] = qr[m] = s4_state(L, m, h); break;
+                    case 4: ql[m] = qr[m] = s4_state(L, m, h, P.nscheme == 42); break;
                     case 5: ql[m] = s5_left(L, m, h); qr[m] = s5_right(L, m, h); break;
                     default: ql[m] = qwl_preright(L, ql_, P.nscheme, m, h); qr[m] = s6_right(L, m, h); break;
                     }
@@ -329,8 +345,9 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
             const InvLine &L = lines[ln];
             const double *f_ = smem + (size_t)ln * LS + work0 + (size_t)10 * H;
             const double *sc = smem + (size_t)ln * LS + work0 + (size_t)15 * H;
-            bool right = P.nscheme == 41 && L.ied < n && l >= n - 2;
-            bool left = P.nscheme == 41 && L.ist > 1 && l <= 3;
+            const bool sections = P.nscheme == 41 || P.nscheme == 42;
+            bool right = sections && L.ied < n && l >= n - 2;
+            bool left = sections && L.ist > 1 && l <= 3;
             long long gi = L.dqbase + (long long)l * L.stride;
             double df;
             if (right) {
