@@ -23,7 +23,9 @@ extern "C" {
 #endif
 
 /* The param.dat namelist values the path reads ($inflow, $step, $flowtype,
- * $technic; read_parameter, PreProcess.f90:80-159). */
+ * $technic; read_parameter, PreProcess.f90:80-159).  Supported: nvis 0 or 1
+ * (laminar), nscheme 4, 41 or 42, nflux 1 (Steger-Warming), 2 (Van Leer) or
+ * 3 (Roe); anything else is rejected with WCNS_ERR_UNSUPPORTED. */
 typedef struct WcnsParams {
     double moo, attack, sideslip, reynolds, tref, twall;
     double cfl, timedt_rate, efix, csrv;
