@@ -6,10 +6,11 @@ Prints one JSON line.  Metric: Mcell-steps/s = points x steps / seconds.
   value  -- device-timed: CUDA events around each step's graph replay on the
             library's stream, inputs resident in HBM; L2 flushed between timed
             steps (256 MiB write, outside the timed region).
-  e2e    -- the public C ABI with host buffers: per step the prim state is
-            copied in from pinned host memory (wcns_set_prim), the step runs
-            (wcns_step), and the updated prim and the residual are copied back
-            (wcns_get_field, wcns_residual).
+  e2e    -- the public C ABI with host buffers: per step the prim state of
+            every block is copied in from pinned host memory
+            (wcns_set_prim_all, ghosted layout), the step runs (wcns_step),
+            and the resulting interior state (wcns_get_flow, flow-file
+            layout) and the residual (wcns_residual) are copied back.
   --impl reference -- the CPU restatement of the reference path (the oracle;
             the Fortran reference cannot be built here) on all host cores.
 N>1 (torchrun): every rank runs its own replica of the case (weak scaling);
@@ -250,15 +251,17 @@ def run_b200(args, rank, world):
         for f, name in enumerate(("r", "u", "v", "w", "p", "t")):
             bufs[f][...] = g.get(name, nb)
         pinned.append(bufs)
+    # results: the interior state of every block in the flow-file layout
+    outs = [[torch.empty((nk, nj, ni), dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
+            for ni, nj, nk in case.dims]
     h2d = sum(6 * a[0].size * 8 for a in pinned)
-    d2h = sum(5 * a[0].size * 8 for a in pinned) + 8 * (2 * case.nblocks + 1)
+    d2h = sum(5 * a[0].size * 8 for a in outs) + 8 * (2 * case.nblocks + 1)
     dist_barrier(world)
     t0 = time.perf_counter()
-    outs = [bufs[:5] for bufs in pinned]
     for _ in range(args.e2e_steps):
         g.set_prim_all(pinned)
         g.step(1, history=False)
-        g.get_prim_all(outs)
+        g.get_flow(outs)
         g.residual_curve()
     e2e_s = time.perf_counter() - t0
     e2e_s = dist_max(e2e_s, world)

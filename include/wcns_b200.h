@@ -80,6 +80,11 @@ int wcns_get_prim(WcnsContext *ctx, int nb, double *r, double *u, double *v, dou
  * wcns_get_prim_all a null t skips T of that block). */
 int wcns_set_prim_all(WcnsContext *ctx, const double *const *prim);
 int wcns_get_prim_all(WcnsContext *ctx, double *const *prim);
+/* The interior primitive state of every block in the flow-file layout of
+ * write_flow_file_parallel (parallel.f90:4073-4145): per block six arrays
+ * of ni*nj*nk doubles (r, u, v, w, p, t; i fastest, no ghost layers), a null
+ * t skipping T of that block.  One synchronisation. */
+int wcns_get_flow(WcnsContext *ctx, double *const *flow);
 int wcns_set_field(WcnsContext *ctx, int field, int nb, const double *in);
 
 /* Per-step drop-ins, in the reference's call order (Main.f90:85-109). */

@@ -181,3 +181,22 @@ def test_all_block_state_transfer():
     for nb in range(1, case.nblocks + 1):
         for x, y in zip(a.get_prim(nb), b.get_prim(nb)):
             assert np.array_equal(x, y)
+
+
+def test_get_flow_is_the_interior():
+    """wcns_get_flow returns each block's interior points in the flow-file
+    layout, exactly the interior of what wcns_get_prim returns."""
+    case = cases.small_plate_case()
+    from wcns_b200.solver import Wcns
+    g = Wcns(case)
+    g.step(2)
+    flow = g.get_flow()
+    for nb in range(1, case.nblocks + 1):
+        full = g.get_prim(nb)
+        for x, y in zip(full, flow[nb - 1]):
+            assert np.array_equal(interior(x, case.dims[nb - 1]), y)
+    five = [[np.zeros_like(a) for a in blk[:5]] for blk in flow]
+    g.get_flow(five)
+    for a, b in zip(five, flow):
+        for x, y in zip(a, b[:5]):
+            assert np.array_equal(x, y)

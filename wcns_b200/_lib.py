@@ -29,6 +29,7 @@ SIGNATURES = {
     "wcns_get_prim": (C.c_int, [_VP, C.c_int] + [_VP] * 6),
     "wcns_set_prim_all": (C.c_int, [_VP, C.POINTER(C.c_void_p)]),
     "wcns_get_prim_all": (C.c_int, [_VP, C.POINTER(C.c_void_p)]),
+    "wcns_get_flow": (C.c_int, [_VP, C.POINTER(C.c_void_p)]),
     "wcns_set_field": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
     "wcns_boundary_all": (C.c_int, [_VP]),
     "wcns_initial_q_dq_c_t": (C.c_int, [_VP]),

@@ -840,6 +840,40 @@ extern "C" int wcns_get_prim_all(WcnsContext *c, double *const *prim) {
     return 0;
 }
 
+// The interior state of every block in the flow-file layout
+// (write_flow_file_parallel, parallel.f90:4073-4145: i = 1..ni fastest,
+// then j, then k, no ghost layers): one strided copy per field and block.
+// flow: 6 pointers per block, r u v w p t; a null t skips T of that block.
+extern "C" int wcns_get_flow(WcnsContext *c, double *const *flow) {
+    if (!c || !flow) { set_err("wcns_get_flow: null argument"); return WCNS_ERR_ARGUMENT; }
+    const int nbk = (int)c->blk.size();
+    for (int b = 0; b < nbk; b++)
+        for (int f = 0; f < 5; f++)
+            if (!flow[6 * b + f]) { set_err("wcns_get_flow: null array"); return WCNS_ERR_ARGUMENT; }
+    CK(cudaEventRecord(c->L.ev_fork, c->stream));
+    cudaStream_t st[3] = {c->stream, c->L.side[0], c->L.side[1]};
+    for (int q = 1; q < 3; q++) CK(cudaStreamWaitEvent(st[q], c->L.ev_fork, 0));
+    int e = 0;
+    for (int b = 0; b < nbk; b++) {
+        const DevBlock &d = c->blk[b].d;
+        for (int f = 0; f < 6; f++) {
+            if (!flow[6 * b + f]) continue;
+            cudaMemcpy3DParms cp = {};
+            // the ghosted box (-2:n+3) starts 3 points before the interior in each direction
+            cp.srcPtr = make_cudaPitchedPtr(c->F.f[F_R + f] + d.off, sizeof(double) * d.gx, d.gx, d.gy);
+            cp.srcPos = make_cudaPos(sizeof(double) * 3, 3, 3);
+            cp.dstPtr = make_cudaPitchedPtr(flow[6 * b + f], sizeof(double) * d.ni, d.ni, d.nj);
+            cp.dstPos = make_cudaPos(0, 0, 0);
+            cp.extent = make_cudaExtent(sizeof(double) * d.ni, d.nj, d.nk);
+            cp.kind = cudaMemcpyDeviceToHost;
+            CK(cudaMemcpy3DAsync(&cp, st[e % 3]));
+            e++;
+        }
+    }
+    for (int q = 0; q < 3; q++) CK(cudaStreamSynchronize(st[q]));
+    return 0;
+}
+
 extern "C" int wcns_set_field(WcnsContext *c, int field, int nb, const double *in) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;

@@ -130,6 +130,26 @@ class Wcns:
         _check(_lib.load().wcns_get_prim_all(self.h, vec))
         return outs
 
+    def get_flow(self, outs=None):
+        """The interior state of every block in the flow-file layout:
+        outs[nb-1] = five or six C-contiguous float64 arrays of shape
+        (nk, nj, ni) for r, u, v, w, p (and T); one synchronisation."""
+        if outs is None:
+            outs = [[np.empty((nk, nj, ni)) for _ in range(6)] for ni, nj, nk in self.dims]
+        if len(outs) != len(self.dims):
+            raise ValueError("one list of five or six arrays per block")
+        ptrs = []
+        for (ni, nj, nk), arrs in zip(self.dims, outs):
+            if len(arrs) not in (5, 6):
+                raise ValueError("five or six arrays per block")
+            for a in arrs:
+                if a.shape != (nk, nj, ni) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError("flow array has the wrong shape, dtype or layout")
+            ptrs += [a.ctypes.data for a in arrs] + ([None] if len(arrs) == 5 else [])
+        vec = (C.c_void_p * len(ptrs))(*ptrs)
+        _check(_lib.load().wcns_get_flow(self.h, vec))
+        return outs
+
     def _checked(self, nb, arrs, n):
         ni, nj, nk = self.dims[nb - 1]
         shape = (nk + 6, nj + 6, ni + 6)
