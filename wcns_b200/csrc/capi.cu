@@ -950,8 +950,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     LaunchCtx &L = c->L;
     int n = 0;
     launch_boundary(L); n += 2;
-    launch_init(L); n += 1;
-    launch_timestep(L); n += 1;
+    launch_init_timestep(L); n += 1;
     if (c->P.nvis == 1) {
         launch_node_derivatives(L); n += 1;
         launch_rhs_dirs(L, true);

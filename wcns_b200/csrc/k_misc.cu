@@ -21,109 +21,114 @@ namespace wcns {
 __device__ __forceinline__ void decode(const DevBlock &B, long long p, int &i, int &j, int &k) { decode_point(B, p, i, j, k); }
 
 // ---------------------------------------------------------------------------
-__global__ void k_init(DevParams P, DevFields F, const DevBlock *__restrict__ blocks, int nblocks) {
-    const int bi = blockIdx.y;
-    const DevBlock B = blocks[bi];
+// initial_q_dq_c_t (sub_tgh.f90:1-32) at one interior point: dq = 0 and, for
+// the viscous path, T and the Sutherland viscosity (plus T on the three
+// ghost layers of the faces the point sits on)
+__device__ __forceinline__ void init_point(const DevParams &P, DevFields &F, const DevBlock &B, int i, int j, int k,
+                                           long long id) {
     const double gama = P.gama, moo2 = P.moo2;
     double *r = F.f[F_R], *p = F.f[F_P], *t = F.f[F_T];
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < B.npts; q += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        decode(B, q, i, j, k);
-        long long id = gidx(B, i, j, k);
 #pragma unroll
-        for (int m = 0; m < 5; m++) F.f[F_DQ1 + m][id] = 0.0;
-        if (P.nvis != 1) continue;
-        t[id] = moo2 * (gama * p[id] / r[id]);
-        F.f[F_VISL][id] = sutherland(P, t[id]);  // compute_visl_ns (GasModel.f90:219-235)
-        // ghost layers of the face this point sits on
-        int dims[3] = {B.ni, B.nj, B.nk};
-        int c[3] = {i, j, k};
-        for (int d = 0; d < 3; d++) {
-            long long st = dstride(B, d);
-            for (int s = 0; s < 2; s++) {
-                if (c[d] != (s ? dims[d] : 1)) continue;
-                long long sg = s ? st : -st;
-                long long i1 = id + sg, i2 = id + 2 * sg, i3 = id + 3 * sg;
-                double a2 = gama * p[i1] / r[i1];
-                t[i1] = moo2 * a2;
-                a2 = gama * p[i2] / r[i2];
-                t[i2] = moo2 * a2;
-                if (d != 0) a2 = gama * p[i3] / fabs(r[i3]);  // i faces reuse a2 (RHS.f90:351-353)
-                t[i3] = moo2 * a2;
-            }
+    for (int m = 0; m < 5; m++) F.f[F_DQ1 + m][id] = 0.0;
+    if (P.nvis != 1) return;
+    t[id] = moo2 * (gama * p[id] / r[id]);
+    F.f[F_VISL][id] = sutherland(P, t[id]);  // compute_visl_ns (GasModel.f90:219-235)
+    // ghost layers of the face this point sits on
+    int dims[3] = {B.ni, B.nj, B.nk};
+    int c[3] = {i, j, k};
+    for (int d = 0; d < 3; d++) {
+        long long st = dstride(B, d);
+        for (int s = 0; s < 2; s++) {
+            if (c[d] != (s ? dims[d] : 1)) continue;
+            long long sg = s ? st : -st;
+            long long i1 = id + sg, i2 = id + 2 * sg, i3 = id + 3 * sg;
+            double a2 = gama * p[i1] / r[i1];
+            t[i1] = moo2 * a2;
+            a2 = gama * p[i2] / r[i2];
+            t[i2] = moo2 * a2;
+            if (d != 0) a2 = gama * p[i3] / fabs(r[i3]);  // i faces reuse a2 (RHS.f90:351-353)
+            t[i3] = moo2 * a2;
         }
     }
 }
 
-void launch_init(const LaunchCtx &c) {
-    long long maxp = 0;
-    for (int b = 0; b < c.nblocks; b++) maxp = c.hblocks[b].npts > maxp ? c.hblocks[b].npts : maxp;
-    dim3 grid((unsigned)((maxp + 255) / 256), c.nblocks);
-    k_init<<<grid, 256, 0, c.stream>>>(*c.P, *c.F, c.blocks, c.nblocks);
+// timestep_tgh (sub_tgh.f90:1270-1348) at one interior point: spectral radii,
+// dtdt and the LU-SGS diagonal coefficient; point-local, reading the point's
+// own T
+__device__ __forceinline__ void timestep_point(const DevParams &P, DevFields &F, long long id) {
+    double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pm = F.f[F_P][id];
+    double cm = sqrt(P.gama * pm / rm);
+    double kx = F.f[F_KCX][id], ky = F.f[F_KCY][id], kz = F.f[F_KCZ][id], kt = 0.0;
+    double ex = F.f[F_ETX][id], ey = F.f[F_ETY][id], ez = F.f[F_ETZ][id], et = 0.0;
+    double cx = F.f[F_CTX][id], cy = F.f[F_CTY][id], cz = F.f[F_CTZ][id], ct = 0.0;
+    double cita = kx * um + ky * vm + kz * wm + kt;
+    double citb = ex * um + ey * vm + ez * wm + et;
+    double citc = cx * um + cy * vm + cz * wm + ct;
+    double cgma = sqrt(kx * kx + ky * ky + kz * kz);
+    double cgmb = sqrt(ex * ex + ey * ey + ez * ez);
+    double cgmc = sqrt(cx * cx + cy * cy + cz * cz);
+    double ra = fabs(cita) + cm * cgma, rb = fabs(citb) + cm * cgmb, rc = fabs(citc) + cm * cgmc;
+    double sva = 0.0, svb = 0.0, svc = 0.0;
+    if (P.nvis == 1 && P.csrv > 0.0) {
+        double rm_vol = rm * F.f[F_VOL][id];
+        double ri = kx * kx + ky * ky + kz * kz;
+        double rj = ex * ex + ey * ey + ez * ez;
+        double rk = cx * cx + cy * cy + cz * cz;
+        double vis = sutherland(P, F.f[F_T][id]);
+        double coef = 2.0 * vis / (P.reynolds * rm_vol + SMALL);
+        double coef1 = P.csrv * coef;
+        sva = coef1 * ri;
+        svb = coef1 * rj;
+        svc = coef1 * rk;
+    }
+    F.f[F_SRA][id] = ra;
+    F.f[F_SRB][id] = rb;
+    F.f[F_SRC][id] = rc;
+    F.f[F_SRVA][id] = sva;
+    F.f[F_SRVB][id] = svb;
+    F.f[F_SRVC][id] = svc;
+    double rv = sva + svb + svc;
+    double rabc = ra + rb + rc + rv;
+    double dt;
+    if (P.timedt_rate > SMALL) {
+        double a = P.cfl / rabc, b = P.timedt_rate / F.f[F_VOL][id];
+        dt = a < b ? a : b;
+    } else {
+        dt = P.cfl / rabc;
+    }
+    F.f[F_DTDT][id] = dt;
+    double rad_ns = ra + rb + rc;
+    if (P.nvis == 1) rad_ns = rad_ns + sva + svb + svc;
+    double ctt = 1.0 / dt;
+    F.f[F_COED][id] = 1.0 / (ctt + 1.0 * 1.0 * rad_ns);
 }
 
-// ---------------------------------------------------------------------------
-__global__ void k_timestep(DevParams P, DevFields F, const DevBlock *__restrict__ blocks, int nblocks) {
+template <bool INIT, bool TIMESTEP>
+__global__ void k_init_timestep(DevParams P, DevFields F, const DevBlock *__restrict__ blocks, int nblocks) {
     const int bi = blockIdx.y;
     const DevBlock B = blocks[bi];
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < B.npts; q += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         decode(B, q, i, j, k);
         long long id = gidx(B, i, j, k);
-        double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pm = F.f[F_P][id];
-        double cm = sqrt(P.gama * pm / rm);
-        double kx = F.f[F_KCX][id], ky = F.f[F_KCY][id], kz = F.f[F_KCZ][id], kt = 0.0;
-        double ex = F.f[F_ETX][id], ey = F.f[F_ETY][id], ez = F.f[F_ETZ][id], et = 0.0;
-        double cx = F.f[F_CTX][id], cy = F.f[F_CTY][id], cz = F.f[F_CTZ][id], ct = 0.0;
-        double cita = kx * um + ky * vm + kz * wm + kt;
-        double citb = ex * um + ey * vm + ez * wm + et;
-        double citc = cx * um + cy * vm + cz * wm + ct;
-        double cgma = sqrt(kx * kx + ky * ky + kz * kz);
-        double cgmb = sqrt(ex * ex + ey * ey + ez * ez);
-        double cgmc = sqrt(cx * cx + cy * cy + cz * cz);
-        double ra = fabs(cita) + cm * cgma, rb = fabs(citb) + cm * cgmb, rc = fabs(citc) + cm * cgmc;
-        double sva = 0.0, svb = 0.0, svc = 0.0;
-        if (P.nvis == 1 && P.csrv > 0.0) {
-            double rm_vol = rm * F.f[F_VOL][id];
-            double ri = kx * kx + ky * ky + kz * kz;
-            double rj = ex * ex + ey * ey + ez * ez;
-            double rk = cx * cx + cy * cy + cz * cz;
-            double vis = sutherland(P, F.f[F_T][id]);
-            double coef = 2.0 * vis / (P.reynolds * rm_vol + SMALL);
-            double coef1 = P.csrv * coef;
-            sva = coef1 * ri;
-            svb = coef1 * rj;
-            svc = coef1 * rk;
-        }
-        F.f[F_SRA][id] = ra;
-        F.f[F_SRB][id] = rb;
-        F.f[F_SRC][id] = rc;
-        F.f[F_SRVA][id] = sva;
-        F.f[F_SRVB][id] = svb;
-        F.f[F_SRVC][id] = svc;
-        double rv = sva + svb + svc;
-        double rabc = ra + rb + rc + rv;
-        double dt;
-        if (P.timedt_rate > SMALL) {
-            double a = P.cfl / rabc, b = P.timedt_rate / F.f[F_VOL][id];
-            dt = a < b ? a : b;
-        } else {
-            dt = P.cfl / rabc;
-        }
-        F.f[F_DTDT][id] = dt;
-        double rad_ns = ra + rb + rc;
-        if (P.nvis == 1) rad_ns = rad_ns + sva + svb + svc;
-        double ctt = 1.0 / dt;
-        F.f[F_COED][id] = 1.0 / (ctt + 1.0 * 1.0 * rad_ns);
+        if (INIT) init_point(P, F, B, i, j, k, id);
+        if (TIMESTEP) timestep_point(P, F, id);
     }
 }
 
-void launch_timestep(const LaunchCtx &c) {
+template <bool INIT, bool TIMESTEP>
+static void launch_init_timestep_t(const LaunchCtx &c) {
     long long maxp = 0;
     for (int b = 0; b < c.nblocks; b++) maxp = c.hblocks[b].npts > maxp ? c.hblocks[b].npts : maxp;
     dim3 grid((unsigned)((maxp + 255) / 256), c.nblocks);
-    k_timestep<<<grid, 256, 0, c.stream>>>(*c.P, *c.F, c.blocks, c.nblocks);
+    k_init_timestep<INIT, TIMESTEP><<<grid, 256, 0, c.stream>>>(*c.P, *c.F, c.blocks, c.nblocks);
 }
+
+void launch_init(const LaunchCtx &c) { launch_init_timestep_t<true, false>(c); }
+void launch_timestep(const LaunchCtx &c) { launch_init_timestep_t<false, true>(c); }
+// both at once, as the step runs them back to back: every value the time
+// step reads at a point is the point's own, written just before
+void launch_init_timestep(const LaunchCtx &c) { launch_init_timestep_t<true, true>(c); }
 
 // ---------------------------------------------------------------------------
 // update_limited: pass A (parallel) + ordered fix-up of non-physical points

@@ -138,6 +138,7 @@ int rhs_vis_max_lines();           // lines per CTA in k_rhs_vis
 void launch_boundary(const LaunchCtx &c);
 void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);
+void launch_init_timestep(const LaunchCtx &c);
 void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
 void launch_lhs(const LaunchCtx &c);
 int setup_sweep(LaunchCtx &c, int cluster, int fine);
