@@ -49,7 +49,10 @@ enum {
     WCNS_F_DQ1, WCNS_F_DQ2, WCNS_F_DQ3, WCNS_F_DQ4, WCNS_F_DQ5,
     WCNS_F_DTDT, WCNS_F_SRA, WCNS_F_SRB, WCNS_F_SRC, WCNS_F_SRVA, WCNS_F_SRVB, WCNS_F_SRVC,
     WCNS_F_KCX, WCNS_F_KCY, WCNS_F_KCZ, WCNS_F_ETX, WCNS_F_ETY, WCNS_F_ETZ,
-    WCNS_F_CTX, WCNS_F_CTY, WCNS_F_CTZ, WCNS_F_VOL
+    WCNS_F_CTX, WCNS_F_CTY, WCNS_F_CTZ, WCNS_F_VOL,
+    /* the Spalart-Allmaras model's fields, present after wcns_sa_setup:
+     * qke (the model variable), vist (eddy viscosity), the wall distance */
+    WCNS_F_QKE, WCNS_F_VIST, WCNS_F_DIST
 };
 
 /* Pre-processing.  Replaces read_bc_parallel + analyze_bc + set_bc_index
@@ -98,6 +101,24 @@ int wcns_lhs(WcnsContext *ctx);                 /* l_h_s_tgh (LHS.f90:1-34) */
 int wcns_communicate_pv(WcnsContext *ctx);      /* communicate_pv_npp (parallel.f90:3166-3215) */
 int wcns_residual(WcnsContext *ctx, double *res_per_block, double *resmax_per_block, double *rms);
                                                 /* residual_curve (PostProcess.f90:1195-1347) */
+
+/* Spalart-Allmaras turbulence model: turbulence(nb) -> differential_model_
+ * turbulence (turblence.f90:15-103), called per block at the start of
+ * r_h_s_vis (RHS.f90:22), for nlamtur=1, nameturb='SA', ncmpcor<=9, ndes=0,
+ * ntrans=0, nwtmax=0.
+ * wcns_sa_setup: allocates the model's arrays, computes the wall distance
+ * (calc_wall_dists_parallel, parallel.f90:4313-4470) from xyz (as for
+ * wcns_create), sets qke and vist to their free-stream values over the
+ * points -1..n+1 (init_SA, turblence.f90:2701-2733) and keeps timedt_turb
+ * ($step) and kmaxlim ($turbulence; <= 1e-15 for no clamp).  Needs nvis 1.
+ * wcns_turbulence: one model step on every block (source, diffusion,
+ * spectral radius, convection, scalar LU-SGS, update of qke at the
+ * interior points 2..n-1, vist at 1..n, kmaxlim clamp at 0..n), reading the
+ * current prim, visl and dtdt.  The ghost values of qke are the caller's
+ * (set with wcns_set_field): the model's boundary conditions and the use of
+ * vist in the mean-flow viscous flux are not part of this library. */
+int wcns_sa_setup(WcnsContext *ctx, const double *const *xyz, double timedt_turb, double kmaxlim);
+int wcns_turbulence(WcnsContext *ctx);
 
 /* Wall force and moment coefficients: force (PostProcess.f90:1415-1480) with
  * force_dif / getforce (1505-1824), over all bctype-2 regions.

@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libwcns_oracle.so")
 
 FIELDS = ["r", "u", "v", "w", "p", "t", "dq1", "dq2", "dq3", "dq4", "dq5", "dtdt", "sra", "srb", "src",
           "srva", "srvb", "srvc", "kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz", "vol",
-          "c", "visl", "q1", "q2", "q3", "q4", "q5"]
+          "qke", "vist", "dist", "c", "visl", "q1", "q2", "q3", "q4", "q5"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 
 
@@ -45,7 +45,8 @@ def lib():
         L.orc_destroy.argtypes = [C.c_void_p]
         L.orc_last_error.restype = C.c_char_p
         for fn in ("orc_boundary_all", "orc_initial_q_dq_c_t", "orc_timestep", "orc_rhs_vis",
-                   "orc_communicate_dq", "orc_rhs_invis", "orc_lhs", "orc_communicate_pv", "orc_n_multipoints"):
+                   "orc_communicate_dq", "orc_rhs_invis", "orc_lhs", "orc_communicate_pv", "orc_n_multipoints",
+                   "orc_turbulence"):
             getattr(L, fn).argtypes = [C.c_void_p]
             getattr(L, fn).restype = C.c_int
         L.orc_set_prim.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 6
@@ -141,3 +142,8 @@ class Oracle:
 
     def n_multipoints(self):
         return lib().orc_n_multipoints(self.h)
+
+    def sa_setup(self, timedt_turb=1.0, kmaxlim=0.0):
+        L = lib()
+        L.orc_sa_setup.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        assert L.orc_sa_setup(self.h, timedt_turb, kmaxlim) == 0

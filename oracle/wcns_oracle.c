@@ -62,6 +62,9 @@ typedef struct {
     double *fld[F_NFIELDS];
     double *rhs[5];
     double *vist;
+    /* Spalart-Allmaras model (allocated by orc_sa_setup): qke, the wall
+     * distance and the model's work arrays */
+    double *qke, *dist, *dqke, *spec, *viseq, *dmu[3];
     int nreg;
     Reg *reg;
     int *bcindex;
@@ -78,6 +81,8 @@ typedef struct {
     int *comp_first, *comp_n;
     int *mem_nb, *mem_i, *mem_j, *mem_k;
     double **snap; /* per block snapshot buffer, 6 fields x ng */
+    int sa;        /* 1 after orc_sa_setup */
+    double timedt_turb, kmaxlim;
 } Orc;
 
 #define IX(B, i, j, k) ((size_t)((i) + 2) + (size_t)(B)->gx * ((size_t)((j) + 2) + (size_t)(B)->gy * (size_t)((k) + 2)))
@@ -1096,6 +1101,8 @@ void orc_destroy(void *h) {
         for (int f = 0; f < F_NFIELDS; f++) free(b->fld[f]);
         for (int m = 0; m < 5; m++) free(b->rhs[m]);
         free(b->vist);
+        free(b->qke); free(b->dist); free(b->dqke); free(b->spec); free(b->viseq);
+        for (int c = 0; c < 3; c++) free(b->dmu[c]);
         for (int c = 0; c < 3; c++) free(b->xyz[c]);
         for (int nr = 0; nr < b->nreg; nr++) { free(b->reg[nr].image); free(b->reg[nr].jmage); free(b->reg[nr].kmage); }
         free(b->reg);
@@ -1120,16 +1127,32 @@ int orc_set_prim(void *h, int nb, const double *r, const double *u, const double
     memcpy(b->fld[F_T], t, b->ng * 8);
     return 0;
 }
+/* field numbers past the path's 28 fields: the SA model's qke, vist and wall
+ * distance (present after orc_sa_setup), then c, visl, q1..q5 */
+enum { F_X_QKE = 28, F_X_VIST = 29, F_X_DIST = 30, F_X_C = 31 };
+static double *field_ptr(const Orc *o, Blk *b, int field) {
+    if (field >= 0 && field <= F_VOL) return b->fld[field];
+    if (field >= F_X_C && field < F_X_C + (F_NFIELDS - F_C)) return b->fld[F_C + (field - F_X_C)];
+    if (!o->sa) return NULL;
+    if (field == F_X_QKE) return b->qke;
+    if (field == F_X_VIST) return b->vist;
+    if (field == F_X_DIST) return b->dist;
+    return NULL;
+}
 int orc_get_field(void *h, int field, int nb, double *out) {
     Orc *o = h;
-    if (nb < 1 || nb > o->nb || field < 0 || field >= F_NFIELDS) return -1;
-    memcpy(out, o->b[nb].fld[field], o->b[nb].ng * 8);
+    if (nb < 1 || nb > o->nb) return -1;
+    double *f = field_ptr(o, &o->b[nb], field);
+    if (!f) return -1;
+    memcpy(out, f, o->b[nb].ng * 8);
     return 0;
 }
 int orc_set_field(void *h, int field, int nb, const double *in) {
     Orc *o = h;
-    if (nb < 1 || nb > o->nb || field < 0 || field >= F_NFIELDS) return -1;
-    memcpy(o->b[nb].fld[field], in, o->b[nb].ng * 8);
+    if (nb < 1 || nb > o->nb) return -1;
+    double *f = field_ptr(o, &o->b[nb], field);
+    if (!f) return -1;
+    memcpy(f, in, o->b[nb].ng * 8);
     return 0;
 }
 
@@ -2461,6 +2484,385 @@ int orc_forces(void *h, const double *ref, double *out) {
     out[6] = out[1] * cosa - out[0] * sina;
     out[7] = cosb * (out[1] * sina + out[0] * cosa) + sinb * out[2];
     out[8] = copysign(1.0, out[1]) * out[5] / (fabs(out[1]) + 1.0e-38);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Spalart-Allmaras model: turbulence -> differential_model_turbulence */
+/* (turblence.f90:15-103) with nlamtur=1, nameturb='SA', ncmpcor<=9,   */
+/* ndes=0, ntrans=0, nwtmax=0 and method=1 (finite differences).       */
+/* ------------------------------------------------------------------ */
+/* model constants, cal_rhs_source_SA turblence.f90:2508-2513 */
+#define SA_CB1 0.1355
+#define SA_CB2 0.622
+#define SA_CV1 7.1
+#define SA_EPS 1.0e-20
+#define SA_CGA (2. / 3.0)
+#define SA_KI 0.419
+#define SA_CW2 0.3
+#define SA_CW3 2.0
+#define SA_MUOO 1.0e-1 /* inflow_turbulence, turblence.f90:3174 */
+#define SA_MINLIM 1.0e-20 /* update_turbulence, turblence.f90:589 */
+
+/* calc_wall_dists_parallel, parallel.f90:4313-4470: squared distance to the
+ * nearest point of any bctype 2, 20 or 21 region (all blocks), then
+ * sqrt + small, over the block's points 1..n */
+static void sa_wall_distance(Orc *o) {
+    size_t nw = 0;
+    for (int nb = 1; nb <= o->nb; nb++)
+        for (int r = 0; r < o->b[nb].nreg; r++) {
+            const Reg *rg = &o->b[nb].reg[r];
+            if (rg->bctype == 2 || rg->bctype == 20 || rg->bctype == 21)
+                nw += (size_t)(rg->s_ed[0] - rg->s_st[0] + 1) * (rg->s_ed[1] - rg->s_st[1] + 1) * (rg->s_ed[2] - rg->s_st[2] + 1);
+        }
+    double *wp = malloc((nw ? nw : 1) * 3 * sizeof(double));
+    size_t m = 0;
+    for (int nb = 1; nb <= o->nb; nb++) {
+        const Blk *b = &o->b[nb];
+        for (int r = 0; r < b->nreg; r++) {
+            const Reg *rg = &b->reg[r];
+            if (!(rg->bctype == 2 || rg->bctype == 20 || rg->bctype == 21)) continue;
+            for (int k = rg->s_st[2]; k <= rg->s_ed[2]; k++)
+                for (int j = rg->s_st[1]; j <= rg->s_ed[1]; j++)
+                    for (int i = rg->s_st[0]; i <= rg->s_ed[0]; i++) {
+                        size_t g = (size_t)(i - 1) + (size_t)b->ni * ((size_t)(j - 1) + (size_t)b->nj * (k - 1));
+                        for (int c = 0; c < 3; c++) wp[3 * m + c] = b->xyz[c][g];
+                        m++;
+                    }
+        }
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int nb = 1; nb <= o->nb; nb++) {
+        Blk *b = &o->b[nb];
+        for (int k = 1; k <= b->nk; k++)
+            for (int j = 1; j <= b->nj; j++)
+                for (int i = 1; i <= b->ni; i++) {
+                    size_t g = (size_t)(i - 1) + (size_t)b->ni * ((size_t)(j - 1) + (size_t)b->nj * (k - 1));
+                    double xc = b->xyz[0][g], yc = b->xyz[1][g], zc = b->xyz[2][g];
+                    double d = 1.0e30;
+                    for (size_t w = 0; w < nw; w++) {
+                        double dx = xc - wp[3 * w], dy = yc - wp[3 * w + 1], dz = zc - wp[3 * w + 2];
+                        double dist = dx * dx + dy * dy + dz * dz;
+                        d = dist < d ? dist : d;
+                    }
+                    b->dist[IX(b, i, j, k)] = sqrt(d) + SMALL;
+                }
+    }
+    free(wp);
+}
+
+/* init_SA, turblence.f90:2701-2733: qke = muoo, vist = muoo*fv1(muoo) over
+ * -1..n+1 */
+static void sa_init(Blk *b, double cv13) {
+    double kafan = SA_MUOO;
+    double kf3 = pow(kafan, 3.0);
+    double fv1 = kf3 / (kf3 + cv13);
+    double vt = SA_MUOO * fv1;
+    for (int k = -1; k <= b->nk + 1; k++)
+        for (int j = -1; j <= b->nj + 1; j++)
+            for (int i = -1; i <= b->ni + 1; i++) {
+                b->qke[IX(b, i, j, k)] = SA_MUOO;
+                b->vist[IX(b, i, j, k)] = vt;
+            }
+}
+
+int orc_sa_setup(void *h, double timedt_turb, double kmaxlim) {
+    Orc *o = h;
+    const double cv13 = pow(SA_CV1, 3.0);
+    for (int nb = 1; nb <= o->nb; nb++) {
+        Blk *b = &o->b[nb];
+        if (!b->qke) {
+            b->qke = calloc(b->ng, sizeof(double));
+            b->dist = calloc(b->ng, sizeof(double));
+            b->dqke = calloc(b->ng, sizeof(double));
+            b->spec = calloc(b->ng, sizeof(double));
+            b->viseq = calloc(b->ng, sizeof(double));
+            for (int c = 0; c < 3; c++) b->dmu[c] = calloc(b->ng, sizeof(double));
+        }
+        sa_init(b, cv13);
+    }
+    o->timedt_turb = timedt_turb;
+    o->kmaxlim = kmaxlim;
+    o->sa = 1;
+    sa_wall_distance(o);
+    return 0;
+}
+
+/* dfidxyz_center, turblence.f90:753-849 (finite-difference branch) at one
+ * point: central differences along i, j, k mapped to x, y, z */
+static void sa_center_deriv(const Blk *b, const double *fi, int i, int j, int k, double *d) {
+    size_t id = IX(b, i, j, k);
+    double dkc = fi[IX(b, i + 1, j, k)] - fi[IX(b, i - 1, j, k)];
+    double det = fi[IX(b, i, j + 1, k)] - fi[IX(b, i, j - 1, k)];
+    double dct = fi[IX(b, i, j, k + 1)] - fi[IX(b, i, j, k - 1)];
+    double *const *f = b->fld;
+    double ddx = dkc * f[F_KCX][id] + det * f[F_ETX][id] + dct * f[F_CTX][id];
+    double ddy = dkc * f[F_KCY][id] + det * f[F_ETY][id] + dct * f[F_CTY][id];
+    double ddz = dkc * f[F_KCZ][id] + det * f[F_ETZ][id] + dct * f[F_CTZ][id];
+    double vol2 = 0.5 / f[F_VOL][id];
+    d[0] = ddx * vol2;
+    d[1] = ddy * vol2;
+    d[2] = ddz * vol2;
+}
+
+/* minmod, Convect.f90:1281-1286 */
+static double minmod(double x, double y) {
+    return 0.5 * (copysign(1.0, x) + copysign(1.0, y)) * fmin(fabs(x), fabs(y));
+}
+
+/* flux_turbulence, turblence.f90:437-459 */
+static double sa_flux(const double *prim, double nx, double ny, double nz, int npn) {
+    double l1 = nx * prim[1] + ny * prim[2] + nz * prim[3];
+    l1 = 0.5 * (l1 + (double)npn * sqrt(l1 * l1));
+    return l1 * prim[4] * prim[0];
+}
+
+/* mxdq_std_turbulence, turblence.f90:560-583 */
+static double sa_mxdq(const double *prim, const double *g, double dq, int npn) {
+    double l1 = g[0] * prim[1] + g[1] * prim[2] + g[2] * prim[3];
+    l1 = 0.5 * (l1 + (double)npn * fabs(l1));
+    return l1 * dq;
+}
+
+static void sa_block(const Orc *o, Blk *b) {
+    const int ni = b->ni, nj = b->nj, nk = b->nk;
+    const int n3[3] = {ni, nj, nk};
+    const double reynolds = o->reynolds, re = 1.0 / reynolds;
+    const double cv13 = pow(SA_CV1, 3.0), ki2 = SA_KI * SA_KI, cw36 = pow(SA_CW3, 6.0), onesix = 1.0 / 6.0;
+    const double cw1 = SA_CB1 / SA_KI / SA_KI + (1.0 + SA_CB2) / SA_CGA;
+    const double ft2 = 0.0;
+    double *const *f = b->fld;
+    /* set_dq_to_zero_turbulence, turblence.f90:270-289 */
+    memset(b->dqke, 0, b->ng * sizeof(double));
+    memset(b->spec, 0, b->ng * sizeof(double));
+    /* cal_rhs_source_SA, turblence.f90:2506-2699: derivatives of qke over 1..n
+     * (those of u, v, w are taken where they are used) */
+    for (int k = 1; k <= nk; k++)
+        for (int j = 1; j <= nj; j++)
+            for (int i = 1; i <= ni; i++) {
+                double d[3];
+                sa_center_deriv(b, b->qke, i, j, k, d);
+                for (int c = 0; c < 3; c++) b->dmu[c][IX(b, i, j, k)] = d[c];
+            }
+    for (int k = 2; k <= nk - 1; k++)
+        for (int j = 2; j <= nj - 1; j++)
+            for (int i = 2; i <= ni - 1; i++) {
+                size_t id = IX(b, i, j, k);
+                double du[3], dv[3], dw[3];
+                sa_center_deriv(b, f[F_U], i, j, k, du);
+                sa_center_deriv(b, f[F_V], i, j, k, dv);
+                sa_center_deriv(b, f[F_W], i, j, k, dw);
+                double ro = R(b)[id], volume = f[F_VOL][id], vsl = f[F_VISL][id], vtbar = b->qke[id];
+                double romu = ro * vtbar;
+                double dn = b->dist[id] > re ? b->dist[id] : re;
+                double dn2 = dn * dn;
+                double reki2dn2 = reynolds * ki2 * dn2;
+                double kafan = romu / vsl;
+                double kf3 = pow(kafan, 3.0);
+                double fv1 = kf3 / (kf3 + cv13);
+                double fv2 = 1.0 - kafan / (1.0 + kafan * fv1);
+                double a = du[1] - dv[0], bb = dv[2] - dw[1], c = dw[0] - du[2];
+                double omg = sqrt(a * a + bb * bb + c * c);
+                double sbar = omg + vtbar / reki2dn2 * fv2;
+                sbar = sbar > SA_EPS ? sbar : SA_EPS;
+                double rbar = vtbar / (sbar * reki2dn2);
+                rbar = rbar < 10.0 ? rbar : 10.0;
+                double rbar5 = pow(rbar, 5.0);
+                double gbar = rbar + SA_CW2 * rbar * (rbar5 - 1.0);
+                double gbar6 = pow(gbar, 6.0);
+                double fw = gbar * pow((1.0 + cw36) / (gbar6 + cw36), onesix);
+                double cpmu = SA_CB1 * (1.0 - ft2) * sbar;
+                double cdmu = (cw1 * fw - SA_CB1 * ft2 / ki2) * vtbar / dn2 / reynolds;
+                double sp = cpmu * vtbar, sd = cdmu * vtbar;
+                double dmx = b->dmu[0][id], dmy = b->dmu[1][id], dmz = b->dmu[2][id];
+                double dbar = SA_CB2 / SA_CGA * (dmx * dmx + dmy * dmy + dmz * dmz) * re;
+                b->dqke[id] = b->dqke[id] - ro * (sp - sd + dbar) * volume;
+                double sm = cpmu - 2.0 * cdmu;
+                b->spec[id] = b->spec[id] - (sm < 0.0 ? sm : 0.0) * volume;
+            }
+    /* viscosity_equivalent_SA_r, turblence.f90:2785-2808, over 1..n */
+    for (int k = 1; k <= nk; k++)
+        for (int j = 1; j <= nj; j++)
+            for (int i = 1; i <= ni; i++) {
+                size_t id = IX(b, i, j, k);
+                b->viseq[id] = 1.5 * (f[F_VISL][id] / R(b)[id] + b->qke[id]);
+            }
+    /* cal_rhs_viscous_turbulence_dif_r, turblence.f90:1022-1185: per
+     * direction the half-point fluxes 2..n, differenced into 2..n-1 */
+    for (int d = 0; d < 3; d++) {
+        const double *mx = metric_dir(b, d, 0), *my = metric_dir(b, d, 1), *mz = metric_dir(b, d, 2);
+        for (int k = 2; k <= nk - 1; k++)
+            for (int j = 2; j <= nj - 1; j++)
+                for (int i = 2; i <= ni - 1; i++) {
+                    int c[3] = {i, j, k};
+                    double fvl[2];
+                    for (int h = 0; h < 2; h++) {
+                        int cm[3] = {i, j, k}, cn[3] = {i, j, k};
+                        cm[d] = c[d] + h;      /* half point l = c[d] + h between l-1 and l */
+                        cn[d] = c[d] + h - 1;
+                        size_t im = IX(b, cm[0], cm[1], cm[2]), in = IX(b, cn[0], cn[1], cn[2]);
+                        double nx = 0.5 * (mx[im] + mx[in]);
+                        double ny = 0.5 * (my[im] + my[in]);
+                        double nz = 0.5 * (mz[im] + mz[in]);
+                        double dmudx = b->dmu[0][im] + b->dmu[0][in];
+                        double dmudy = b->dmu[1][im] + b->dmu[1][in];
+                        double dmudz = b->dmu[2][im] + b->dmu[2][in];
+                        double vis = b->viseq[im] + b->viseq[in];
+                        fvl[h] = (dmudx * nx + dmudy * ny + dmudz * nz) * vis * 0.25;
+                    }
+                    size_t id = IX(b, i, j, k);
+                    b->dqke[id] = b->dqke[id] - re * R(b)[id] * (fvl[1] - fvl[0]);
+                }
+    }
+    /* cal_spec_turbulence_r, turblence.f90:218-259 */
+    const double re2 = re * 2.0;
+    for (int k = 2; k <= nk - 1; k++)
+        for (int j = 2; j <= nj - 1; j++)
+            for (int i = 2; i <= ni - 1; i++) {
+                size_t id = IX(b, i, j, k);
+                double u = U(b)[id], v = V(b)[id], w = W(b)[id];
+                double unx = u * f[F_KCX][id] + v * f[F_KCY][id] + w * f[F_KCZ][id];
+                double uny = u * f[F_ETX][id] + v * f[F_ETY][id] + w * f[F_ETZ][id];
+                double unz = u * f[F_CTX][id] + v * f[F_CTY][id] + w * f[F_CTZ][id];
+                b->spec[id] = b->spec[id] + fabs(unx) + fabs(uny) + fabs(unz) + 1.0 / (f[F_DTDT][id] * o->timedt_turb);
+                double nx = f[F_KCX][id] * f[F_KCX][id] + f[F_KCY][id] * f[F_KCY][id] + f[F_KCZ][id] * f[F_KCZ][id];
+                double ny = f[F_ETX][id] * f[F_ETX][id] + f[F_ETY][id] * f[F_ETY][id] + f[F_ETZ][id] * f[F_ETZ][id];
+                double nz = f[F_CTX][id] * f[F_CTX][id] + f[F_CTY][id] * f[F_CTY][id] + f[F_CTZ][id] * f[F_CTZ][id];
+                double vis = b->viseq[id] / f[F_VOL][id];
+                b->spec[id] = b->spec[id] + re2 * vis * (nx + ny + nz);
+            }
+    /* cal_rhs_inviscous_turbulence + NND_turbulence, turblence.f90:291-435,
+     * xk = xb = 0 (never assigned in the reference) */
+    const double xk = 0.0, xb = 0.0, c1 = 0.25 * (1.0 + xk), c2 = 0.25 * (1.0 - xk);
+    for (int d = 0; d < 3; d++) {
+        const int n = n3[d];
+        const double *mx = metric_dir(b, d, 0), *my = metric_dir(b, d, 1), *mz = metric_dir(b, d, 2);
+        const int la = d == 0 ? 1 : 0, lb = d == 2 ? 1 : 2;  /* the two other directions */
+        for (int bq = 2; bq <= n3[lb] - 1; bq++)
+            for (int aq = 2; aq <= n3[la] - 1; aq++) {
+                double *ql = malloc((size_t)(n + 3) * 5 * sizeof(double));   /* l = -1..n+1 */
+                double *dqv = malloc((size_t)(n + 3) * 5 * sizeof(double));
+                double *qcl = malloc((size_t)(n + 3) * 5 * sizeof(double));
+                double *qcr = malloc((size_t)(n + 3) * 5 * sizeof(double));
+                double *fc = malloc((size_t)(n + 3) * sizeof(double));
+#define QL(m, l) ql[5 * ((l) + 1) + (m)]
+#define DQV(m, l) dqv[5 * ((l) + 1) + (m)]
+#define QCL(m, l) qcl[5 * ((l) + 1) + (m)]
+#define QCR(m, l) qcr[5 * ((l) + 1) + (m)]
+                for (int l = 0; l <= n + 1; l++) {
+                    int c[3];
+                    c[d] = l; c[la] = aq; c[lb] = bq;
+                    size_t id = IX(b, c[0], c[1], c[2]);
+                    QL(0, l) = R(b)[id]; QL(1, l) = U(b)[id]; QL(2, l) = V(b)[id]; QL(3, l) = W(b)[id];
+                    QL(4, l) = b->qke[id];
+                }
+                for (int l = 1; l <= n + 1; l++)
+                    for (int m = 0; m < 5; m++) DQV(m, l) = QL(m, l) - QL(m, l - 1);
+                for (int l = 1; l <= n; l++)
+                    for (int m = 0; m < 5; m++) {
+                        QCL(m, l) = minmod(xb * DQV(m, l + 1), DQV(m, l));
+                        QCR(m, l) = minmod(DQV(m, l + 1), xb * DQV(m, l));
+                    }
+                for (int l = 2; l <= n; l++) {
+                    int c0[3], c1i[3];
+                    c0[d] = l - 1; c0[la] = aq; c0[lb] = bq;
+                    c1i[d] = l; c1i[la] = aq; c1i[lb] = bq;
+                    size_t i0 = IX(b, c0[0], c0[1], c0[2]), i1 = IX(b, c1i[0], c1i[1], c1i[2]);
+                    double nx = 0.50 * (mx[i0] + mx[i1]);
+                    double ny = 0.50 * (my[i0] + my[i1]);
+                    double nz = 0.50 * (mz[i0] + mz[i1]);
+                    double dql[5], dqr[5];
+                    for (int m = 0; m < 5; m++) {
+                        dql[m] = QL(m, l - 1) + c1 * QCR(m, l - 1) + c2 * QCL(m, l - 1);
+                        dqr[m] = QL(m, l) - c1 * QCL(m, l) - c2 * QCR(m, l);
+                    }
+                    double fl = sa_flux(dql, nx, ny, nz, 1);
+                    double fr = sa_flux(dqr, nx, ny, nz, -1);
+                    fc[l] = fl + fr;
+                }
+                for (int l = 2; l <= n - 1; l++) {
+                    int c[3];
+                    c[d] = l; c[la] = aq; c[lb] = bq;
+                    size_t id = IX(b, c[0], c[1], c[2]);
+                    b->dqke[id] = b->dqke[id] + (fc[l + 1] - fc[l]);
+                }
+#undef QL
+#undef DQV
+#undef QCL
+#undef QCR
+                free(ql); free(dqv); free(qcl); free(qcr); free(fc);
+            }
+    }
+    /* lusgs_turbulence, turblence.f90:477-558 */
+    for (int k = 2; k <= nk - 1; k++)
+        for (int j = 2; j <= nj - 1; j++)
+            for (int i = 2; i <= ni - 1; i++) {
+                double rhs0 = 0.0, t[3];
+                for (int d = 0; d < 3; d++) {
+                    int c[3] = {i, j, k};
+                    c[d] -= 1;
+                    double prim[5], g[4];
+                    getprim(b, c[0], c[1], c[2], prim);
+                    getrkec(b, c[0], c[1], c[2], d, g);
+                    t[d] = sa_mxdq(prim, g, b->dqke[IX(b, c[0], c[1], c[2])], 1);
+                }
+                rhs0 = t[0] + t[1] + t[2];
+                size_t id = IX(b, i, j, k);
+                b->dqke[id] = (rhs0 - b->dqke[id]) / b->spec[id];
+            }
+    for (int k = nk - 1; k >= 2; k--)
+        for (int j = nj - 1; j >= 2; j--)
+            for (int i = ni - 1; i >= 2; i--) {
+                double rhs0, t[3];
+                for (int d = 0; d < 3; d++) {
+                    int c[3] = {i, j, k};
+                    c[d] += 1;
+                    double prim[5], g[4];
+                    getprim(b, c[0], c[1], c[2], prim);
+                    getrkec(b, c[0], c[1], c[2], d, g);
+                    t[d] = sa_mxdq(prim, g, b->dqke[IX(b, c[0], c[1], c[2])], -1);
+                }
+                rhs0 = t[0] + t[1] + t[2];
+                size_t id = IX(b, i, j, k);
+                b->dqke[id] = b->dqke[id] - rhs0 / b->spec[id];
+            }
+    /* update_turbulence, turblence.f90:585-623 */
+    for (int k = 2; k <= nk - 1; k++)
+        for (int j = 2; j <= nj - 1; j++)
+            for (int i = 2; i <= ni - 1; i++) {
+                size_t id = IX(b, i, j, k);
+                double qn = b->qke[id] + b->dqke[id] / R(b)[id], lim = SA_MINLIM * SA_MUOO;
+                b->qke[id] = qn > lim ? qn : lim;
+            }
+    /* cal_vist_SA, turblence.f90:2735-2760, over 1..n */
+    for (int k = 1; k <= nk; k++)
+        for (int j = 1; j <= nj; j++)
+            for (int i = 1; i <= ni; i++) {
+                size_t id = IX(b, i, j, k);
+                double romu = R(b)[id] * b->qke[id];
+                double kafan = romu / f[F_VISL][id];
+                double kf3 = pow(kafan, 3.0);
+                double fv1 = kf3 / (kf3 + cv13);
+                b->vist[id] = romu * fv1;
+            }
+    /* max_control_turbulence, turblence.f90:625-660, over 0..n (layer 0 of
+     * visl is never computed: compute_visl_ns covers 1..n) */
+    if (o->kmaxlim > 1.0e-15)
+        for (int k = 0; k <= nk; k++)
+            for (int j = 0; j <= nj; j++)
+                for (int i = 0; i <= ni; i++) {
+                    size_t id = IX(b, i, j, k);
+                    double lim = o->kmaxlim * f[F_VISL][id];
+                    b->vist[id] = b->vist[id] < lim ? b->vist[id] : lim;
+                }
+}
+
+/* turbulence(nb) for every block (RHS.f90:22 inside r_h_s_vis) */
+int orc_turbulence(void *h) {
+    Orc *o = h;
+    if (!o->sa) { set_err("orc_turbulence: orc_sa_setup was not called"); return 1; }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int nb = 1; nb <= o->nb; nb++) sa_block(o, &o->b[nb]);
     return 0;
 }
 

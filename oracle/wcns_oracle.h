@@ -56,6 +56,15 @@ int orc_n_multipoints(void *h);
  * out = {cfx, cfy, cfz, cmx, cmy, cmz, cl, cd, xcp} */
 int orc_forces(void *h, const double *ref, double *out);
 
+/* Spalart-Allmaras model (turbulence, turblence.f90:15-103; nlamtur=1,
+ * nameturb='SA', ncmpcor<=9, ndes=0, ntrans=0, nwtmax=0).  orc_sa_setup
+ * computes the wall distance (calc_wall_dists_parallel, parallel.f90:
+ * 4313-4470), applies init_SA (turblence.f90:2701-2733) and keeps
+ * timedt_turb and kmaxlim; fields 28, 29, 30 (qke, vist, wall distance) are
+ * then readable and writable, and orc_turbulence runs the model step. */
+int orc_sa_setup(void *h, double timedt_turb, double kmaxlim);
+int orc_turbulence(void *h);
+
 /* line-operator hooks used by the known-answer tests */
 void orc_value_half_node(int n, int ni, const double *q, double *qh);
 void orc_flux_dxyz(int nl, int ni, const double *f, double *df);

@@ -1,0 +1,191 @@
+"""Spalart-Allmaras model (turbulence -> differential_model_turbulence,
+turblence.f90:15-103): oracle known-answer tests on the CPU and GPU parity
+through the C ABI.
+
+GPU and oracle evaluate pow() in the source term and in fv1 (CUDA's and
+glibc's results may differ in the last bit), so qke and vist are compared
+with a relative bar of 1e-12; the wall distance is an exact minimum and must
+agree bitwise."""
+import numpy as np
+import pytest
+
+from tests.helpers import compare_fields, interior, with_params
+from wcns_b200 import cases
+
+TOL = 1e-12
+MUOO = 0.1
+CV13 = 7.1 ** 3.0
+
+
+def wall_points(case):
+    pts = []
+    for nb, (x, y, z) in enumerate(case.xyz, start=1):
+        for r in case.regions:
+            if r[0] != nb or r[7] not in (2, 20, 21):
+                continue
+            lo = [min(abs(r[1 + 2 * d]), abs(r[2 + 2 * d])) for d in range(3)]
+            hi = [max(abs(r[1 + 2 * d]), abs(r[2 + 2 * d])) for d in range(3)]
+            sl = (slice(lo[2] - 1, hi[2]), slice(lo[1] - 1, hi[1]), slice(lo[0] - 1, hi[0]))
+            pts.append(np.stack([x[sl].ravel(), y[sl].ravel(), z[sl].ravel()], axis=1))
+    return np.concatenate(pts) if pts else np.zeros((0, 3))
+
+
+def test_oracle_wall_distance(oracle_lib):
+    """calc_wall_dists_parallel: sqrt of the minimum squared distance to any
+    point of a bctype 2/20/21 region, plus small, at every point 1..n."""
+    case = cases.small_plate_case()
+    o = oracle_lib.Oracle(case)
+    o.sa_setup()
+    w = wall_points(case)
+    assert len(w) > 0
+    for nb, (x, y, z) in enumerate(case.xyz, start=1):
+        p = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+        dx = p[:, None, 0] - w[None, :, 0]
+        dy = p[:, None, 1] - w[None, :, 1]
+        dz = p[:, None, 2] - w[None, :, 2]
+        d2 = (dx * dx + dy * dy + dz * dz).min(axis=1)
+        want = (np.sqrt(d2) + 1.0e-38).reshape(x.shape)
+        got = interior(o.get("dist", nb), o.dims[nb - 1])
+        np.testing.assert_array_equal(got, want)
+
+
+def test_oracle_sa_init(oracle_lib):
+    """init_SA: qke = muoo and vist = muoo*fv1(muoo) over -1..n+1."""
+    case = cases.small_plate_case()
+    o = oracle_lib.Oracle(case)
+    o.sa_setup()
+    kf3 = MUOO ** 3.0
+    vt = MUOO * (kf3 / (kf3 + CV13))
+    for nb in range(1, len(o.dims) + 1):
+        ni, nj, nk = o.dims[nb - 1]
+        q, v = o.get("qke", nb), o.get("vist", nb)
+        sl = (slice(1, nk + 4), slice(1, nj + 4), slice(1, ni + 4))  # points -1..n+1
+        assert np.all(q[sl] == MUOO)
+        assert np.all(v[sl] == vt)
+
+
+def sa_at_rest(r, qk, visl, vol, dtdt, dist, metr, reynolds, timedt_turb):
+    """One model step for a fluid at rest with uniform qke, written out
+    independently: the derivatives of qke and the velocity vanish, so the
+    diffusion and convection terms and all LU-SGS off-diagonal products are
+    zero; what remains is the source term, the diagonal (spec) and the
+    update (turblence.f90:2567-2686, 218-259, 477-558, 585-623)."""
+    cb1, cb2, cga, ki, cw2, cw3 = 0.1355, 0.622, 2.0 / 3.0, 0.419, 0.3, 2.0
+    ki2, cw36, onesix = ki * ki, cw3 ** 6.0, 1.0 / 6.0
+    cw1 = cb1 / ki / ki + (1.0 + cb2) / cga
+    re = 1.0 / reynolds
+    dn = np.where(dist > re, dist, re)
+    dn2 = dn * dn
+    reki2dn2 = (reynolds * ki2) * dn2
+    kafan = (r * qk) / visl
+    kf3 = np.power(kafan, 3.0)
+    fv1 = kf3 / (kf3 + CV13)
+    fv2 = 1.0 - kafan / (1.0 + kafan * fv1)
+    sbar = 0.0 + (qk / reki2dn2) * fv2
+    sbar = np.where(sbar > 1.0e-20, sbar, 1.0e-20)
+    rbar = qk / (sbar * reki2dn2)
+    rbar = np.where(rbar < 10.0, rbar, 10.0)
+    gbar = rbar + (cw2 * rbar) * (np.power(rbar, 5.0) - 1.0)
+    fw = gbar * np.power((1.0 + cw36) / (np.power(gbar, 6.0) + cw36), onesix)
+    cpmu = cb1 * sbar
+    cdmu = (cw1 * fw - 0.0) * qk / dn2 / reynolds
+    dq = 0.0 - (r * ((cpmu * qk - cdmu * qk) + 0.0)) * vol
+    sm = cpmu - 2.0 * cdmu
+    spec = 0.0 - np.where(sm < 0.0, sm, 0.0) * vol
+    spec = spec + 0.0 + 0.0 + 0.0 + 1.0 / (dtdt * timedt_turb)
+    viseq = 1.5 * (visl / r + qk)
+    ss = [metr[3 * d] * metr[3 * d] + metr[3 * d + 1] * metr[3 * d + 1] + metr[3 * d + 2] * metr[3 * d + 2]
+          for d in range(3)]
+    spec = spec + ((re * 2.0) * (viseq / vol)) * ((ss[0] + ss[1]) + ss[2])
+    dq = (0.0 - dq) / spec
+    qn = qk + dq / r
+    return np.where(qn > 1.0e-21, qn, 1.0e-21)
+
+
+def test_oracle_sa_at_rest(oracle_lib):
+    case = cases.small_plate_case()
+    o = oracle_lib.Oracle(case)
+    for nb in range(1, len(o.dims) + 1):
+        z = np.zeros_like(o.get("u", nb))
+        for n in ("u", "v", "w"):
+            o.set(n, nb, z)
+    o.phase("initial_q_dq_c_t")
+    o.phase("timestep")
+    o.sa_setup(timedt_turb=2.0)
+    o.phase("turbulence")
+    names = ["kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz"]
+    for nb in range(1, len(o.dims) + 1):
+        ni, nj, nk = o.dims[nb - 1]
+        c = (slice(4, nk + 2), slice(4, nj + 2), slice(4, ni + 2))  # interior points 2..n-1
+        g = {n: o.get(n, nb)[c] for n in ["r", "visl", "vol", "dtdt", "dist"] + names}
+        want = sa_at_rest(g["r"], MUOO, g["visl"], g["vol"], g["dtdt"], g["dist"], [g[n] for n in names],
+                          case.params.reynolds, 2.0)
+        np.testing.assert_allclose(o.get("qke", nb)[c], want, rtol=1e-14, atol=0)
+        # vist follows qke at the interior points (cal_vist_SA)
+        romu = g["r"] * o.get("qke", nb)[c]
+        kf3 = np.power(romu / g["visl"], 3.0)
+        np.testing.assert_allclose(o.get("vist", nb)[c], romu * (kf3 / (kf3 + CV13)), rtol=1e-14, atol=0)
+
+
+# --------------------------------------------------------------------------
+# GPU parity
+
+def _pair(case):
+    from oracle.pyoracle import Oracle
+    from wcns_b200.solver import Wcns
+    return Wcns(case), Oracle(case)
+
+
+SA_CASES = {
+    "plate_small": lambda: cases.small_plate_case(),
+    "plate_small_sym2d": lambda: cases.small_plate_case(nk=4),
+    "plate_small_roe42": lambda: cases.small_plate_case(nscheme=42),
+    # no wall: the distance stays at its 1e30 start (sqrt 1e15)
+    "vortex_viscous": lambda: with_params(cases.vortex_case(ni=33, nj=17, nk=9, nscheme=41, nflux=3), nvis=1),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kmaxlim", [0.0, 3.0e-7])
+@pytest.mark.parametrize("name", list(SA_CASES))
+def test_sa_parity(name, kmaxlim):
+    case = SA_CASES[name]()
+    g, o = _pair(case)
+    g.boundary_all(); o.phase("boundary_all")
+    g.initial_q_dq_c_t(); o.phase("initial_q_dq_c_t")
+    g.timestep_tgh(); o.phase("timestep")
+    g.sa_setup(1.5, kmaxlim); o.sa_setup(1.5, kmaxlim)
+    e = compare_fields(g, o, ["dist", "qke", "vist"], region="all")
+    assert max(e.values()) == 0.0, e
+    # a seeded non-uniform qke (ghosts included) so that every term is active
+    rng = np.random.default_rng(11)
+    for nb in range(1, len(o.dims) + 1):
+        q = MUOO * (1.0 + 0.3 * rng.random(o.get("qke", nb).shape))
+        g.set("qke", nb, q); o.set("qke", nb, q)
+    q0 = o.get("qke", 1)
+    for step in range(3):
+        g.turbulence(); o.phase("turbulence")
+        e = compare_fields(g, o, ["qke", "vist"], region="all")
+        assert max(e.values()) <= TOL, (step, e)
+    # the model moved qke
+    d = o.dims[0]
+    assert np.max(np.abs(interior(o.get("qke", 1), d) - interior(q0, d))) > 0
+
+
+@pytest.mark.gpu
+def test_sa_errors():
+    from wcns_b200.solver import Wcns, WcnsError
+    g = Wcns(cases.small_plate_case())
+    with pytest.raises(WcnsError) as ei:
+        g.turbulence()
+    assert ei.value.code == 1
+    with pytest.raises(WcnsError) as ei:
+        g.get("qke", 1)
+    assert ei.value.code == 5
+    with pytest.raises(WcnsError) as ei:
+        g.sa_setup(0.0)
+    assert ei.value.code == 1
+    e = Wcns(cases.vortex_case(ni=17, nj=9, nk=9))  # inviscid: no visl
+    with pytest.raises(WcnsError) as ei:
+        e.sa_setup()
+    assert ei.value.code == 5

@@ -47,6 +47,8 @@ SIGNATURES = {
     "wcns_launches_per_step": (C.c_int, [_VP]),
     "wcns_n_multipoints": (C.c_int, [_VP]),
     "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
+    "wcns_sa_setup": (C.c_int, [_VP, C.POINTER(C.c_void_p), C.c_double, C.c_double]),
+    "wcns_turbulence": (C.c_int, [_VP]),
     "wcns_residual_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p), _VP, _VP, _VP, _VP]),
 }
 

@@ -95,6 +95,10 @@ struct WcnsContext {
     int hist_cap = 0;
     cudaGraphExec_t graph = nullptr;
     int nmulti = 0;
+    // Spalart-Allmaras model (wcns_sa_setup)
+    double *sa_pool = nullptr;
+    SaFields SA{};
+    SaParams SAP{};
     int launches = 0;
     ~WcnsContext() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -106,6 +110,7 @@ struct WcnsContext {
         for (void *p : owned) cudaFree(p);
         if (pool) cudaFree(pool);
         if (pm_pool) cudaFree(pm_pool);
+        if (sa_pool) cudaFree(sa_pool);
         if (stream) cudaStreamDestroy(stream);
     }
     template <class T>
@@ -764,12 +769,24 @@ extern "C" int wcns_set_prim(WcnsContext *c, int nb, const double *r, const doub
     return 0;
 }
 
+// device base of a public field: the path's fields, and the SA model's
+// qke, vist and wall distance once wcns_sa_setup has run
+static double *field_base(WcnsContext *c, int field) {
+    if (field >= 0 && field <= WCNS_F_VOL) return c->F.f[field];
+    if (!c->sa_pool) return nullptr;
+    if (field == WCNS_F_QKE) return c->SA.qke;
+    if (field == WCNS_F_VIST) return c->SA.vist;
+    if (field == WCNS_F_DIST) return c->SA.dist;
+    return nullptr;
+}
+
 extern "C" int wcns_get_field(WcnsContext *c, int field, int nb, double *out) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;
-    if (field < 0 || field > WCNS_F_VOL || !out) { set_err("wcns_get_field: unsupported field"); return WCNS_ERR_UNSUPPORTED; }
+    double *base = field_base(c, field);
+    if (!base || !out) { set_err("wcns_get_field: unsupported field"); return WCNS_ERR_UNSUPPORTED; }
     size_t n = (size_t)d->gx * d->gy * d->gz;
-    CK(cudaMemcpyAsync(out, c->F.f[field] + d->off, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out, base + d->off, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return 0;
 }
@@ -877,10 +894,84 @@ extern "C" int wcns_get_flow(WcnsContext *c, double *const *flow) {
 extern "C" int wcns_set_field(WcnsContext *c, int field, int nb, const double *in) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;
-    if (field < 0 || field > WCNS_F_VOL || !in) { set_err("wcns_set_field: unsupported field"); return WCNS_ERR_UNSUPPORTED; }
+    double *base = field_base(c, field);
+    if (!base || !in) { set_err("wcns_set_field: unsupported field"); return WCNS_ERR_UNSUPPORTED; }
     size_t n = (size_t)d->gx * d->gy * d->gz;
-    CK(cudaMemcpyAsync(c->F.f[field] + d->off, in, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(base + d->off, in, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+// Spalart-Allmaras model set-up: the model's arrays, the wall distance of
+// calc_wall_dists_parallel (parallel.f90:4313-4470; wall points: every point
+// of the bctype 2, 20 and 21 regions) and init_SA (turblence.f90:2701-2733).
+extern "C" int wcns_sa_setup(WcnsContext *c, const double *const *xyz, double timedt_turb, double kmaxlim) {
+    if (!c || !xyz) { set_err("wcns_sa_setup: null argument"); return WCNS_ERR_ARGUMENT; }
+    const int nbk = (int)c->blk.size();
+    for (int q = 0; q < 3 * nbk; q++)
+        if (!xyz[q]) { set_err("wcns_sa_setup: missing coordinates"); return WCNS_ERR_ARGUMENT; }
+    if (c->P.nvis != 1) { set_err("wcns_sa_setup: the SA model needs the viscous path (nvis 1)"); return WCNS_ERR_UNSUPPORTED; }
+    if (!(timedt_turb > 0.0)) { set_err("wcns_sa_setup: timedt_turb must be positive"); return WCNS_ERR_ARGUMENT; }
+    if (!c->sa_pool) {
+        CK(cudaMalloc(&c->sa_pool, sizeof(double) * SA_NFIELDS * (size_t)c->total));
+        CK(cudaMemset(c->sa_pool, 0, sizeof(double) * SA_NFIELDS * (size_t)c->total));
+        double *f[SA_NFIELDS];
+        for (int q = 0; q < SA_NFIELDS; q++) f[q] = c->sa_pool + (size_t)q * c->total;
+        c->SA = SaFields{f[0], f[1], f[2], f[3], f[4], {f[5], f[6], f[7]}};
+    }
+    // constants as cal_rhs_source_SA evaluates its parameter statements
+    const double cb1 = 0.1355, cb2 = 0.622, cv1 = 7.1, cga = 2. / 3.0, ki = 0.419, cw3 = 2.0;
+    SaParams &S = c->SAP;
+    S.reynolds = c->P.reynolds;
+    S.re = c->P.re;
+    S.ki2 = ki * ki;
+    S.cv13 = pow(cv1, 3.0);
+    S.cw36 = pow(cw3, 6.0);
+    S.onesix = 1.0 / 6.0;
+    S.cw1 = cb1 / ki / ki + (1.0 + cb2) / cga;
+    S.timedt_turb = timedt_turb;
+    S.kmaxlim = kmaxlim;
+    c->L.SA = &c->SA;
+    c->L.SAP = &c->SAP;
+    // coordinates in the pool's layout and the wall point list
+    std::vector<double> wall, tmp;
+    double *xyzd = nullptr, *walld = nullptr;
+    CK(cudaMalloc(&xyzd, sizeof(double) * 3 * (size_t)c->total));
+    for (int b = 0; b < nbk; b++) {
+        const DevBlock &d = c->blk[b].d;
+        tmp.assign((size_t)d.gx * d.gy * d.gz, 0.0);
+        for (int q = 0; q < 3; q++) {
+            const double *src = xyz[3 * b + q];
+            for (int k = 1; k <= d.nk; k++)
+                for (int j = 1; j <= d.nj; j++)
+                    for (int i = 1; i <= d.ni; i++)
+                        tmp[gidx(d, i, j, k) - d.off] = src[(i - 1) + (size_t)d.ni * ((j - 1) + (size_t)d.nj * (k - 1))];
+            cudaMemcpy(xyzd + (size_t)q * c->total + d.off, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice);
+        }
+        for (const HReg &R : c->blk[b].regs) {
+            if (!(R.bctype == 2 || R.bctype == 20 || R.bctype == 21)) continue;
+            for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                    for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                        size_t g = (size_t)(i - 1) + (size_t)d.ni * ((size_t)(j - 1) + (size_t)d.nj * (k - 1));
+                        for (int q = 0; q < 3; q++) wall.push_back(xyz[3 * b + q][g]);
+                    }
+        }
+    }
+    if (wall.size() / 3 > 0x7fffffff) { cudaFree(xyzd); set_err("wcns_sa_setup: too many wall points"); return WCNS_ERR_ARGUMENT; }
+    if (!wall.empty()) {
+        cudaError_t e = cudaMalloc(&walld, sizeof(double) * wall.size());
+        if (e == cudaSuccess) e = cudaMemcpy(walld, wall.data(), sizeof(double) * wall.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { cudaFree(xyzd); cudaFree(walld); set_err(std::string("wcns_sa_setup: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
+    }
+    // init_SA: vt = muoo * fv1(muoo)
+    const double muoo = 1.0e-1, kf3 = pow(muoo, 3.0), vt = muoo * (kf3 / (kf3 + S.cv13));
+    launch_sa_setup(c->L, xyzd, walld, (int)(wall.size() / 3), vt);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(xyzd);
+    if (walld) cudaFree(walld);
+    if (e != cudaSuccess) { set_err(std::string("wcns_sa_setup: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
     return 0;
 }
 
@@ -900,6 +991,10 @@ PHASE(wcns_rhs_vis, if (c->P.nvis == 1) {
     launch_rhs_dirs(c->L, true);
 })
 PHASE(wcns_communicate_dq, launch_communicate(c->L, 0))
+PHASE(wcns_turbulence, {
+    if (!c->sa_pool) { set_err("wcns_turbulence: wcns_sa_setup was not called"); return WCNS_ERR_ARGUMENT; }
+    launch_turbulence(c->L);
+})
 PHASE(wcns_rhs_invis, launch_rhs_dirs(c->L, false))
 PHASE(wcns_lhs, {
     launch_lhs(c->L);

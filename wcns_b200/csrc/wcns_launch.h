@@ -46,6 +46,20 @@ struct DevWall {
     long long quad_off;  // first quad in the quad array
 };
 
+// Spalart-Allmaras model arrays (one field each, the pool's layout): qke,
+// vist, the wall distance, and the model's dqke, spec and qke derivatives
+struct SaFields {
+    double *qke, *vist, *dist, *dqke, *spec, *dmu[3];
+};
+constexpr int SA_NFIELDS = 8;
+
+// SA constants as the reference evaluates them (cal_rhs_source_SA,
+// turblence.f90:2508-2513), computed on the host, and the $step/$turbulence
+// values timedt_turb and kmaxlim
+struct SaParams {
+    double reynolds, re, ki2, cv13, cw36, onesix, cw1, timedt_turb, kmaxlim;
+};
+
 struct LaunchCtx {
     cudaStream_t stream = 0;
     long long total = 0;               // points of the field pool (stride of a field)
@@ -99,6 +113,9 @@ struct LaunchCtx {
     // update bad-point lists
     int *bad_count = nullptr;       // per block
     long long *bad_list = nullptr;  // per block, capacity BAD_CAP
+    // Spalart-Allmaras model (after wcns_sa_setup)
+    const SaFields *SA = nullptr;
+    const SaParams *SAP = nullptr;
 };
 
 constexpr int BAD_CAP = 512;
@@ -147,5 +164,9 @@ void launch_forces(const LaunchCtx &c, double xref, double yref, double zref);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
 int setup_residual(int nblocks, int ctas);  // -1 when the block count is too large
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
+// SA model: set-up (init_SA and the wall distance; xyz: 3 fields of the
+// pool's layout, wall: 3 doubles per wall point) and one model step
+void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, int nwall, double vt);
+void launch_turbulence(const LaunchCtx &c);
 
 }  // namespace wcns

@@ -16,7 +16,8 @@ import numpy as np
 from . import _lib
 
 FIELDS = ["r", "u", "v", "w", "p", "t", "dq1", "dq2", "dq3", "dq4", "dq5", "dtdt", "sra", "srb", "src",
-          "srva", "srvb", "srvc", "kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz", "vol"]
+          "srva", "srvb", "srvc", "kcx", "kcy", "kcz", "etx", "ety", "etz", "ctx", "cty", "ctz", "vol",
+          "qke", "vist", "dist"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 FORCE_KEYS = ("cfx", "cfy", "cfz", "cmx", "cmy", "cmz", "cl", "cd", "xcp")
 
@@ -58,6 +59,7 @@ class Wcns:
         _check(L.wcns_create(C.byref(self._prm), len(self.dims), dims, xyz_p, regs.shape[0],
                              regs.ctypes.data_as(C.POINTER(C.c_int)), C.byref(h)))
         self.h = h
+        self._xyz = (keep, xyz_p)
         for nb, prim in enumerate(case.prim, start=1):
             self.set_prim(nb, prim)
 
@@ -188,6 +190,16 @@ class Wcns:
 
     def communicate_pv_npp(self):
         _check(_lib.load().wcns_communicate_pv(self.h))
+
+    # -- Spalart-Allmaras model (turblence.f90) ----------------------------
+    def sa_setup(self, timedt_turb=1.0, kmaxlim=0.0):
+        """Model arrays, wall distance (calc_wall_dists_parallel) and init_SA;
+        fields "qke", "vist", "dist" become readable and writable."""
+        _check(_lib.load().wcns_sa_setup(self.h, self._xyz[1], timedt_turb, kmaxlim))
+
+    def turbulence(self):
+        """turbulence(nb) for every block (RHS.f90:22)."""
+        _check(_lib.load().wcns_turbulence(self.h))
 
     def residual_curve(self):
         nb = len(self.dims)
