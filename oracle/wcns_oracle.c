@@ -1530,6 +1530,7 @@ static void spect_point(Orc *o, Blk *b, int i, int j, int k, int ii, int jj, int
             double rj = ex * ex + ey * ey + ez * ez;
             double rk = cx * cx + cy * cy + cz * cz;
             double vis = b->fld[F_VISL][ic];
+            if (o->sa) vis = vis + b->vist[ic]; /* spectvist, LHS.f90:141-241 */
             double coef = 2.0 * vis / (o->reynolds * rm_vol + SMALL);
             double coef1 = o->prm.csrv * coef;
             b->fld[F_SRVA][id] = coef1 * ri;
@@ -1926,9 +1927,16 @@ static void rhs_vis_block(Orc *o, Blk *b) {
     free(duv);
 }
 
+static void sa_block(const Orc *o, Blk *b);
 int orc_rhs_vis(void *h) {
     Orc *o = h;
     if (o->prm.nvis != 1) return 0;
+    /* turbulence(nb) at the start of r_h_s_vis (RHS.f90:22); a block's model
+     * step reads only that block, so all blocks can go first */
+    if (o->sa) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int nb = 1; nb <= o->nb; nb++) sa_block(o, &o->b[nb]);
+    }
     for (int nb = 1; nb <= o->nb; nb++) rhs_vis_block(o, &o->b[nb]);
     return 0;
 }

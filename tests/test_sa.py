@@ -173,6 +173,36 @@ def test_sa_parity(name, kmaxlim):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["plate_small", "plate_small_sym2d"])
+def test_sa_coupled(name):
+    """With the model set up, the time step uses visl + vist (spectvist,
+    LHS.f90:141-241), r_h_s_vis runs turbulence(nb) first (RHS.f90:22) and
+    the viscous flux uses visl + vist and visl*cp/prl + vist*cp/prt; then
+    whole steps through the step graph."""
+    case = SA_CASES[name]()
+    g, o = _pair(case)
+    g.sa_setup(1.0, 0.0); o.sa_setup(1.0, 0.0)
+    rng = np.random.default_rng(5)
+    for nb in range(1, len(o.dims) + 1):
+        q = MUOO * (1.0 + 50.0 * rng.random(o.get("qke", nb).shape))  # eddy viscosity of the order of visl
+        g.set("qke", nb, q); o.set("qke", nb, q)
+    g.boundary_all(); o.phase("boundary_all")
+    g.initial_q_dq_c_t(); o.phase("initial_q_dq_c_t")
+    g.timestep_tgh(); o.phase("timestep")
+    e = compare_fields(g, o, ["dtdt", "srva", "srvb", "srvc"])
+    assert max(e.values()) <= TOL, e
+    g.r_h_s_vis(); o.phase("rhs_vis")
+    e = compare_fields(g, o, ["qke", "vist"], region="all")
+    e.update(compare_fields(g, o, ["dq1", "dq2", "dq3", "dq4", "dq5"]))
+    assert max(e.values()) <= TOL, e
+    hg = g.step(3)
+    ho = o.step(3)
+    np.testing.assert_allclose(hg, ho, rtol=1e-10, atol=0)
+    e = compare_fields(g, o, ["r", "u", "v", "w", "p", "qke", "vist"])
+    assert max(e.values()) <= 1e-10, e
+
+
+@pytest.mark.gpu
 def test_sa_errors():
     from wcns_b200.solver import Wcns, WcnsError
     g = Wcns(cases.small_plate_case())

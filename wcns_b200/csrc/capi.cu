@@ -616,10 +616,11 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
         return WCNS_ERR_CUDA;
     }
     // field pool
-    size_t bytes = sizeof(double) * (size_t)F_NALL * (size_t)c->total;
+    size_t bytes = sizeof(double) * (size_t)F_NPOOL * (size_t)c->total;
     if (cudaMalloc(&c->pool, bytes) != cudaSuccess) { delete c; set_err("device allocation of the field pool failed"); return WCNS_ERR_CUDA; }
     cudaMemset(c->pool, 0, bytes);
-    for (int f = 0; f < F_NALL; f++) c->F.f[f] = c->pool + (size_t)f * c->total;
+    for (int f = 0; f < F_NPOOL; f++) c->F.f[f] = c->pool + (size_t)f * c->total;
+    c->F.f[F_VIST] = nullptr;
     // sweep arrays, plane-major: dq (5 planes of values), the static records
     // (SR_N per cell) and three dynamic records (DYN_N per cell); the memset
     // leaves zero the records that no kernel ever writes
@@ -933,6 +934,14 @@ extern "C" int wcns_sa_setup(WcnsContext *c, const double *const *xyz, double ti
     S.kmaxlim = kmaxlim;
     c->L.SA = &c->SA;
     c->L.SAP = &c->SAP;
+    // the mean-flow kernels now read vist (spectvist, the viscous
+    // coefficients); a step graph captured before holds the old arguments
+    c->F.f[F_VIST] = c->SA.vist;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    c->launches = 0;
     // coordinates in the pool's layout and the wall point list
     std::vector<double> wall, tmp;
     double *xyzd = nullptr, *walld = nullptr;
@@ -987,6 +996,7 @@ PHASE(wcns_boundary_all, launch_boundary(c->L))
 PHASE(wcns_initial_q_dq_c_t, launch_init(c->L))
 PHASE(wcns_timestep, launch_timestep(c->L))
 PHASE(wcns_rhs_vis, if (c->P.nvis == 1) {
+    if (c->sa_pool) launch_turbulence(c->L);  // turbulence(nb), RHS.f90:22
     launch_node_derivatives(c->L);
     launch_rhs_dirs(c->L, true);
 })
@@ -1047,6 +1057,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     launch_boundary(L); n += 2;
     launch_init_timestep(L); n += 1;
     if (c->P.nvis == 1) {
+        if (c->sa_pool) { launch_turbulence(L); n += 4; }
         launch_node_derivatives(L); n += 1;
         launch_rhs_dirs(L, true);
         for (int d = 0; d < 3; d++) n += L.vis[d].ngroups ? 1 : 0;

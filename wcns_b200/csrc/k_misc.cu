@@ -75,6 +75,7 @@ __device__ __forceinline__ void timestep_point(const DevParams &P, DevFields &F,
         double rj = ex * ex + ey * ey + ez * ez;
         double rk = cx * cx + cy * cy + cz * cz;
         double vis = sutherland(P, F.f[F_T][id]);
+        if (F.f[F_VIST]) vis = vis + F.f[F_VIST][id];  // spectvist, LHS.f90:141-241
         double coef = 2.0 * vis / (P.reynolds * rm_vol + SMALL);
         double coef1 = P.csrv * coef;
         sva = coef1 * ri;

@@ -156,10 +156,11 @@ __global__ void __launch_bounds__(VIS_THREADS, 2) k_rhs_vis(DevParams P, DevFiel
                 v[VS_MET + c] = inner ? __ldg(F.f[F_KCX + 3 * (c % 3) + c / 3] + gi) : 0.0;
             v[VS_VOL] = inner ? __ldg(F.f[F_VOL] + gi) : 0.0;
             // viscosity at the point, as the reference's visl/vist arrays:
-            // mu + vist and mu*cp_prl + vist*cp_prt with vist = 0 (laminar)
+            // mu + vist and mu*cp_prl + vist*cp_prt (vist = 0 when laminar)
             const double mu = inner ? sutherland(P, v[VS_U + 3]) : 0.0;
-            v[VS_V1] = inner ? mu + 0.0 : 0.0;
-            v[VS_V2] = inner ? mu * P.cp_prl + 0.0 * P.cp_prt : 0.0;
+            const double vt = (inner && F.f[F_VIST]) ? __ldg(F.f[F_VIST] + gi) : 0.0;
+            v[VS_V1] = inner ? mu + vt : 0.0;
+            v[VS_V2] = inner ? mu * P.cp_prl + vt * P.cp_prt : 0.0;
             double *S = smem + (size_t)ln * LS + p;
 #pragma unroll
             for (int f = 0; f < VIS_NF; f++) S[f * W] = v[f];

@@ -37,7 +37,11 @@ enum Field : int {
     F_COED,
     F_OLD1, F_OLD2, F_OLD3, F_OLD4, F_OLD5,
     F_DUV0,  // 12 node derivatives of (u,v,w,T): F_DUV0 .. F_DUV0+11
-    F_NALL = F_DUV0 + 12
+    F_NPOOL = F_DUV0 + 12,  // fields of the pool
+    // the SA model's eddy viscosity (its own allocation; null while the
+    // model is not set up, which the kernels read as vist = 0)
+    F_VIST = F_NPOOL,
+    F_NALL
 };
 
 struct DevParams {
