@@ -143,6 +143,10 @@ class Oracle:
     def n_multipoints(self):
         return lib().orc_n_multipoints(self.h)
 
+    def sa_boundary_rules(self, on=True):
+        lib().orc_sa_boundary_rules.argtypes = [C.c_void_p, C.c_int]
+        assert lib().orc_sa_boundary_rules(self.h, 1 if on else 0) == 0
+
     def sa_setup(self, timedt_turb=1.0, kmaxlim=0.0):
         L = lib()
         L.orc_sa_setup.argtypes = [C.c_void_p, C.c_double, C.c_double]

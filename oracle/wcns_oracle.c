@@ -65,6 +65,7 @@ typedef struct {
     /* Spalart-Allmaras model (allocated by orc_sa_setup): qke, the wall
      * distance and the model's work arrays */
     double *qke, *dist, *dqke, *spec, *viseq, *dmu[3];
+    double *sa_snap; /* qke and vist at the start of the BC pass (2 x ng) */
     int nreg;
     Reg *reg;
     int *bcindex;
@@ -82,6 +83,7 @@ typedef struct {
     int *mem_nb, *mem_i, *mem_j, *mem_k;
     double **snap; /* per block snapshot buffer, 6 fields x ng */
     int sa;        /* 1 after orc_sa_setup */
+    int sa_bc;     /* 1: boundary_all also applies the model's qke/vist rules */
     double timedt_turb, kmaxlim;
 } Orc;
 
@@ -1101,7 +1103,7 @@ void orc_destroy(void *h) {
         for (int f = 0; f < F_NFIELDS; f++) free(b->fld[f]);
         for (int m = 0; m < 5; m++) free(b->rhs[m]);
         free(b->vist);
-        free(b->qke); free(b->dist); free(b->dqke); free(b->spec); free(b->viseq);
+        free(b->qke); free(b->dist); free(b->dqke); free(b->spec); free(b->viseq); free(b->sa_snap);
         for (int c = 0; c < 3; c++) free(b->dmu[c]);
         for (int c = 0; c < 3; c++) free(b->xyz[c]);
         for (int nr = 0; nr < b->nreg; nr++) { free(b->reg[nr].image); free(b->reg[nr].jmage); free(b->reg[nr].kmage); }
@@ -1162,6 +1164,15 @@ int orc_set_field(void *h, int field, int nb, const double *in) {
 /* ------------------------------------------------------------------ */
 #define SET5(B, id, a, bb, c, d, e) do { R(B)[id] = (a); U(B)[id] = (bb); V(B)[id] = (c); W(B)[id] = (d); P(B)[id] = (e); } while (0)
 
+#define SA_MUOO_BC 1.0e-1 /* muoo, inflow_turbulence turblence.f90:3174 */
+
+/* The SA model's one-layer boundary rules for qke and vist, applied when
+ * o->sa_bc is set, point by point where the reference calls them inside each
+ * BC routine.  F: face point, G: first ghost, T: interior neighbour. */
+#define SA_BC(o) ((o)->sa && (o)->sa_bc)
+/* BC_face_dif_turbulence, turblence.f90:2255-2267: face <- (T + G) / 2 */
+static void sa_face_dif(Blk *b, size_t f, size_t g, size_t t) { b->qke[f] = 0.5 * (b->qke[t] + b->qke[g]); }
+
 /* boundary_n1_vir3 (Sub2.f90:206-322) / boundary_n1_vir3_other
  * (parallel.f90:2723-2846): ghost layers from the partner's interior. */
 static void bc_vir3(Orc *o, int nb, Reg *rg) {
@@ -1180,6 +1191,20 @@ static void bc_vir3(Orc *o, int nb, Reg *rg) {
                 int bi = reg_box_index(rg, i, j, k);
                 int it = rg->image[bi], jt = rg->jmage[bi], kt = rg->kmage[bi];
                 int is = i, js = j, ks = k;
+                if (SA_BC(o)) {
+                    /* parallel.f90:2775-2792 (Sub2.f90:262-278 in place): the
+                     * first ghost takes the partner's vist and qke, the face
+                     * point the mean of that ghost and its interior neighbour */
+                    size_t g = IX(b, i + rg->s_lr3d[0], j + rg->s_lr3d[1], k + rg->s_lr3d[2]);
+                    size_t f = IX(b, i, j, k), t = IX(b, i - rg->s_lr3d[0], j - rg->s_lr3d[1], k - rg->s_lr3d[2]);
+                    size_t ps = IX(bt, it - rg->t_lr3d[0], jt - rg->t_lr3d[1], kt - rg->t_lr3d[2]);
+                    const double *pq = same ? bt->qke : o->b[rg->nbt].sa_snap;
+                    const double *pv = same ? bt->vist : o->b[rg->nbt].sa_snap + bt->ng;
+                    b->vist[g] = pv[ps];
+                    b->vist[f] = (b->vist[g] + b->vist[t]) * 0.5;
+                    b->qke[g] = pq[ps];
+                    b->qke[f] = (b->qke[g] + b->qke[t]) * 0.5;
+                }
                 for (int l = 1; l <= 3; l++) {
                     is += rg->s_lr3d[0]; js += rg->s_lr3d[1]; ks += rg->s_lr3d[2];
                     it -= rg->t_lr3d[0]; jt -= rg->t_lr3d[1]; kt -= rg->t_lr3d[2];
@@ -1192,7 +1217,7 @@ static void bc_vir3(Orc *o, int nb, Reg *rg) {
 }
 
 /* dif_average, BC.f90:1972-2008 */
-static void bc_dif_average(Blk *b, Reg *rg) {
+static void bc_dif_average(const Orc *o, Blk *b, Reg *rg) {
     for (int i = rg->s_st[0]; i <= rg->s_ed[0]; i++)
         for (int j = rg->s_st[1]; j <= rg->s_ed[1]; j++)
             for (int k = rg->s_st[2]; k <= rg->s_ed[2]; k++) {
@@ -1204,6 +1229,7 @@ static void bc_dif_average(Blk *b, Reg *rg) {
                 V(b)[f] = 0.5 * (V(b)[s] + V(b)[t]);
                 W(b)[f] = 0.5 * (W(b)[s] + W(b)[t]);
                 P(b)[f] = 0.5 * (P(b)[s] + P(b)[t]);
+                if (SA_BC(o)) sa_face_dif(b, f, s, t);
             }
 }
 
@@ -1221,6 +1247,7 @@ static void bc_symmetry(Orc *o, Blk *b, Reg *rg) {
                     jt = jt < 1 ? 1 : (jt > b->nj ? b->nj : jt);
                     kt = kt < 1 ? 1 : (kt > b->nk ? b->nk : kt);
                     size_t t = IX(b, it, jt, kt);
+                    if (SA_BC(o)) b->qke[IX(b, is, js, ks)] = b->qke[t]; /* BC_symmetry_turbulence, BC.f90:269 */
                     double rm = R(b)[t], um = U(b)[t], vm = V(b)[t], wm = -W(b)[t], pm = P(b)[t];
                     SET5(b, IX(b, is, js, ks), rm, um, vm, wm, pm);
                     is += L[0]; js += L[1]; ks += L[2];
@@ -1230,8 +1257,7 @@ static void bc_symmetry(Orc *o, Blk *b, Reg *rg) {
                     wm = 0.0;
                     SET5(b, IX(b, is, js, ks), rm, um, vm, wm, pm);
                 }
-        bc_dif_average(b, rg);
-        (void)o;
+        bc_dif_average(o, b, rg);
         return;
     }
     int ci = (rg->s_st[0] + rg->s_ed[0]) / 2, cj = (rg->s_st[1] + rg->s_ed[1]) / 2, ck = (rg->s_st[2] + rg->s_ed[2]) / 2;
@@ -1249,9 +1275,10 @@ static void bc_symmetry(Orc *o, Blk *b, Reg *rg) {
                     size_t t = IX(b, it, jt, kt), s = IX(b, is, js, ks);
                     double s1 = 2.0 * (nx * U(b)[t] + ny * V(b)[t] + nz * W(b)[t]);
                     SET5(b, s, R(b)[t], U(b)[t] - s1 * nx, V(b)[t] - s1 * ny, W(b)[t] - s1 * nz, P(b)[t]);
+                    if (l == 1 && SA_BC(o)) b->qke[s] = b->qke[t]; /* BC_symmetry_turbulence, BC.f90:416 */
                 }
             }
-    bc_dif_average(b, rg);
+    bc_dif_average(o, b, rg);
 }
 
 /* boundary_4 (far field, Riemann invariants), BC.f90:460-607 */
@@ -1296,6 +1323,20 @@ static void bc_farfield(Orc *o, Blk *b, Reg *rg) {
                     else { rb = o->roo; ub = o->uoo; vb = o->voo; wb = o->woo; pb = o->poo; }
                 }
                 SET5(b, IX(b, i, j, k), rb, ub, vb, wb, pb);
+                if (SA_BC(o)) {
+                    /* BC_farfield_turbulence_tgh, sub_tgh.f90:713-787: the
+                     * sign of the contravariant velocity of the boundary state
+                     * with the face point's metrics picks muoo (inflow) or the
+                     * interior value, for the face point and the first ghost */
+                    size_t f = IX(b, i, j, k);
+                    const double *mx = metric_dir(b, rg->s_nd - 1, 0), *my = metric_dir(b, rg->s_nd - 1, 1),
+                                 *mz = metric_dir(b, rg->s_nd - 1, 2);
+                    double tem_lr = (double)L[rg->s_nd - 1];
+                    double ut = tem_lr * (mx[f] * U(b)[f] + my[f] * V(b)[f] + mz[f] * W(b)[f]);
+                    double qv = ut < 0.0 ? SA_MUOO_BC : b->qke[t];
+                    b->qke[f] = qv;
+                    b->qke[IX(b, i + L[0], j + L[1], k + L[2])] = ut < 0.0 ? SA_MUOO_BC : b->qke[t];
+                }
                 SET5(b, IX(b, i + L[0], j + L[1], k + L[2]), rb, ub, vb, wb, pb);
                 SET5(b, IX(b, i + 2 * L[0], j + 2 * L[1], k + 2 * L[2]), rb, ub, vb, wb, pb);
                 SET5(b, IX(b, i + 3 * L[0], j + 3 * L[1], k + 3 * L[2]), -rb, ub, vb, wb, pb);
@@ -1308,19 +1349,26 @@ static void bc_inflow(Orc *o, Blk *b, Reg *rg) {
     for (int i = rg->s_st[0]; i <= rg->s_ed[0]; i++)
         for (int j = rg->s_st[1]; j <= rg->s_ed[1]; j++)
             for (int k = rg->s_st[2]; k <= rg->s_ed[2]; k++)
-                for (int n = 0; n <= 3; n++)
+                for (int n = 0; n <= 3; n++) {
                     SET5(b, IX(b, i + n * L[0], j + n * L[1], k + n * L[2]), o->roo, o->uoo, o->voo, o->woo, o->poo);
+                    /* BC_farfield_turbulence, BC.f90:638: face and first ghost */
+                    if (n <= 1 && SA_BC(o)) b->qke[IX(b, i + n * L[0], j + n * L[1], k + n * L[2])] = SA_MUOO_BC;
+                }
 }
 
 /* boundary_6 (supersonic outflow), BC.f90:667-749 */
-static void bc_outflow(Blk *b, Reg *rg) {
+static void bc_outflow(const Orc *o, Blk *b, Reg *rg) {
     const int *L = rg->s_lr3d;
     for (int i = rg->s_st[0]; i <= rg->s_ed[0]; i++)
         for (int j = rg->s_st[1]; j <= rg->s_ed[1]; j++)
             for (int k = rg->s_st[2]; k <= rg->s_ed[2]; k++) {
                 size_t t = IX(b, i - L[0], j - L[1], k - L[2]);
                 double rm = R(b)[t], um = U(b)[t], vm = V(b)[t], wm = W(b)[t], pm = P(b)[t];
-                for (int n = 0; n <= 3; n++) SET5(b, IX(b, i + n * L[0], j + n * L[1], k + n * L[2]), rm, um, vm, wm, pm);
+                for (int n = 0; n <= 3; n++) {
+                    SET5(b, IX(b, i + n * L[0], j + n * L[1], k + n * L[2]), rm, um, vm, wm, pm);
+                    /* BC_outflow_turbulence, BC.f90:721: face and first ghost */
+                    if (n <= 1 && SA_BC(o)) b->qke[IX(b, i + n * L[0], j + n * L[1], k + n * L[2])] = b->qke[t];
+                }
             }
 }
 
@@ -1337,6 +1385,7 @@ static void bc_wall(Orc *o, Blk *b, Reg *rg) {
                     size_t t2 = IX(b, i - 2 * L[0], j - 2 * L[1], k - 2 * L[2]);
                     size_t t3 = IX(b, i - 3 * L[0], j - 3 * L[1], k - 3 * L[2]);
                     SET5(b, g1, R(b)[t1], -U(b)[t1], -V(b)[t1], -W(b)[t1], P(b)[t1]);
+                    if (SA_BC(o)) b->qke[g1] = -b->qke[t1]; /* BC_wall_turbulence, BC.f90:1280 */
                     double pres = (4.0 * P(b)[t1] - P(b)[t2]) / 3.0;
                     double tres, dres;
                     if (o->prm.twall > 0.0) {
@@ -1349,6 +1398,7 @@ static void bc_wall(Orc *o, Blk *b, Reg *rg) {
                     }
                     dres = moocp * pres / tres;
                     SET5(b, IX(b, i, j, k), dres, 0.0, 0.0, 0.0, pres);
+                    if (SA_BC(o)) sa_face_dif(b, IX(b, i, j, k), g1, t1); /* BC.f90:1301 */
                     size_t g2 = IX(b, i + 2 * L[0], j + 2 * L[1], k + 2 * L[2]);
                     size_t g3 = IX(b, i + 3 * L[0], j + 3 * L[1], k + 3 * L[2]);
                     SET5(b, g2, R(b)[t2], -U(b)[t2], -V(b)[t2], -W(b)[t2], P(b)[t2]);
@@ -1368,7 +1418,7 @@ static void bc_wall(Orc *o, Blk *b, Reg *rg) {
                         SET5(b, s, rr, U(b)[t] - s1 * nx, V(b)[t] - s1 * ny, W(b)[t] - s1 * nz, P(b)[t]);
                     }
                 }
-        bc_dif_average(b, rg);
+        bc_dif_average(o, b, rg);
     }
 }
 
@@ -1378,6 +1428,10 @@ int orc_boundary_all(void *h) {
     for (int nb = 1; nb <= o->nb; nb++) {
         Blk *b = &o->b[nb];
         for (int f = 0; f < 5; f++) memcpy(o->snap[nb] + f * b->ng, b->fld[F_R + f], b->ng * 8);
+        if (SA_BC(o)) {
+            memcpy(b->sa_snap, b->qke, b->ng * 8);
+            memcpy(b->sa_snap + b->ng, b->vist, b->ng * 8);
+        }
     }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int nb = 1; nb <= o->nb; nb++) {
@@ -1389,7 +1443,7 @@ int orc_boundary_all(void *h) {
             case 3: bc_symmetry(o, b, rg); break;
             case 4: bc_farfield(o, b, rg); break;
             case 5: bc_inflow(o, b, rg); break;
-            case 6: bc_outflow(b, rg); break;
+            case 6: bc_outflow(o, b, rg); break;
             default: bc_vir3(o, nb, rg); break;
             }
         }
@@ -2585,6 +2639,7 @@ int orc_sa_setup(void *h, double timedt_turb, double kmaxlim) {
             b->dqke = calloc(b->ng, sizeof(double));
             b->spec = calloc(b->ng, sizeof(double));
             b->viseq = calloc(b->ng, sizeof(double));
+            b->sa_snap = calloc(2 * b->ng, sizeof(double));
             for (int c = 0; c < 3; c++) b->dmu[c] = calloc(b->ng, sizeof(double));
         }
         sa_init(b, cv13);
@@ -2866,6 +2921,11 @@ static void sa_block(const Orc *o, Blk *b) {
 }
 
 /* turbulence(nb) for every block (RHS.f90:22 inside r_h_s_vis) */
+int orc_sa_boundary_rules(void *h, int on) {
+    ((Orc *)h)->sa_bc = on ? 1 : 0;
+    return 0;
+}
+
 int orc_turbulence(void *h) {
     Orc *o = h;
     if (!o->sa) { set_err("orc_turbulence: orc_sa_setup was not called"); return 1; }

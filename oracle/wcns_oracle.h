@@ -64,6 +64,10 @@ int orc_forces(void *h, const double *ref, double *out);
  * then readable and writable, and orc_turbulence runs the model step. */
 int orc_sa_setup(void *h, double timedt_turb, double kmaxlim);
 int orc_turbulence(void *h);
+/* on != 0: orc_boundary_all also applies the model's one-layer qke/vist
+ * rules of every BC routine (BC_*_turbulence, the interface copies and face
+ * means).  Off by default: the CUDA path does not apply them yet. */
+int orc_sa_boundary_rules(void *h, int on);
 
 /* line-operator hooks used by the known-answer tests */
 void orc_value_half_node(int n, int ni, const double *q, double *qh);

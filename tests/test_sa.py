@@ -9,7 +9,7 @@ agree bitwise."""
 import numpy as np
 import pytest
 
-from tests.helpers import compare_fields, interior, with_params
+from tests.helpers import compare_fields, interior, supersonic_box_case, with_params
 from wcns_b200 import cases
 
 TOL = 1e-12
@@ -125,6 +125,102 @@ def test_oracle_sa_at_rest(oracle_lib):
         romu = g["r"] * o.get("qke", nb)[c]
         kf3 = np.power(romu / g["visl"], 3.0)
         np.testing.assert_allclose(o.get("vist", nb)[c], romu * (kf3 / (kf3 + CV13)), rtol=1e-14, atol=0)
+
+
+def _region_geometry(r):
+    """Face points of a BC record and its outward direction (s_lr3d)."""
+    rng = [(abs(r[1 + 2 * d]), abs(r[2 + 2 * d])) for d in range(3)]
+    lr = [0, 0, 0]
+    for d in range(3):
+        if rng[d][0] == rng[d][1]:
+            lr[d] = -1 if rng[d][0] == 1 else 1
+            break
+    pts = [(i, j, k) for k in range(min(rng[2]), max(rng[2]) + 1) for j in range(min(rng[1]), max(rng[1]) + 1)
+           for i in range(min(rng[0]), max(rng[0]) + 1)]
+    return pts, lr
+
+
+SA_BC_CASES = {
+    "plate_small": lambda: cases.small_plate_case(),
+    "plate_small_sym2d": lambda: cases.small_plate_case(nk=4),
+    "supersonic_box": lambda: supersonic_box_case(),
+}
+
+
+@pytest.mark.parametrize("name", list(SA_BC_CASES))
+def test_oracle_sa_boundary_rules(oracle_lib, name):
+    """The oracle's restatement of the model's one-layer qke/vist boundary
+    rules (BC_*_turbulence and the interface copies), checked at every face
+    point whose face, first ghost and interior neighbour no other region of
+    the block touches: wall ghost = -interior and face = 0; symmetry ghost =
+    interior and face = the mean; far field face and ghost = muoo where the
+    boundary state flows in, else the interior value; inflow = muoo; outflow
+    = interior; interface face = mean of the copied ghost and the interior."""
+    case = SA_BC_CASES[name]()
+    o = oracle_lib.Oracle(case)
+    o.sa_setup()
+    rng = np.random.default_rng(7)
+    pre_q, pre_v = {}, {}
+    for nb in range(1, len(o.dims) + 1):
+        q = MUOO * (1.0 + rng.random(o.get("qke", nb).shape))
+        v = 1e-6 * (1.0 + rng.random(q.shape))
+        o.set("qke", nb, q); o.set("vist", nb, v)
+        pre_q[nb], pre_v[nb] = q, v
+    # off by default: boundary_all leaves qke alone
+    o.phase("boundary_all")
+    assert all(np.array_equal(o.get("qke", nb), pre_q[nb]) for nb in pre_q)
+    for nb in pre_q:
+        o.set("qke", nb, pre_q[nb]); o.set("vist", nb, pre_v[nb])
+    o.sa_boundary_rules(True)
+    o.phase("boundary_all")
+    checked, ff_sides = {}, set()
+    for nb in range(1, len(o.dims) + 1):
+        regs = [r for r in case.regions if r[0] == nb]
+        touched = {}
+        geo = []
+        for r in regs:
+            pts, lr = _region_geometry(r)
+            geo.append((r, pts, lr))
+            for (i, j, k) in pts:
+                for n in (0, 1):
+                    p = (i + n * lr[0], j + n * lr[1], k + n * lr[2])
+                    touched[p] = touched.get(p, 0) + 1
+        q, v = o.get("qke", nb), o.get("vist", nb)
+        U = [o.get(n, nb) for n in ("u", "v", "w")]
+        A = lambda a, p: a[p[2] + 2, p[1] + 2, p[0] + 2]
+        for r, pts, lr in geo:
+            bt = int(r[7])
+            sd = [d for d in range(3) if lr[d]][0]
+            met = [o.get(n, nb) for n in (("kcx", "kcy", "kcz"), ("etx", "ety", "etz"), ("ctx", "cty", "ctz"))[sd]]
+            for (i, j, k) in pts:
+                f = (i, j, k)
+                g = (i + lr[0], j + lr[1], k + lr[2])
+                t = (i - lr[0], j - lr[1], k - lr[2])
+                if touched.get(f) != 1 or touched.get(g) != 1 or t in touched:
+                    continue
+                qt = A(pre_q[nb], t)
+                if bt == 2:
+                    assert A(q, g) == -qt and A(q, f) == 0.0
+                elif bt == 3:
+                    assert A(q, g) == qt and A(q, f) == 0.5 * (qt + A(q, g))
+                elif bt == 4:
+                    ut = float(lr[sd]) * (A(met[0], f) * A(U[0], f) + A(met[1], f) * A(U[1], f) + A(met[2], f) * A(U[2], f))
+                    want = MUOO if ut < 0.0 else qt
+                    ff_sides.add(ut < 0.0)
+                    assert A(q, f) == want and A(q, g) == want
+                elif bt == 5:
+                    assert A(q, f) == MUOO and A(q, g) == MUOO
+                elif bt == 6:
+                    assert A(q, f) == qt and A(q, g) == qt
+                elif bt == -1:
+                    assert A(q, f) == (A(q, g) + qt) * 0.5
+                    assert A(v, f) == (A(v, g) + A(pre_v[nb], t)) * 0.5
+                checked[bt] = checked.get(bt, 0) + 1
+    types = set(int(x) for x in case.regions[:, 7])
+    assert set(checked) == types, (checked, types)
+    assert min(checked.values()) >= 4, checked
+    if name == "plate_small":
+        assert ff_sides == {True, False}  # both far-field branches seen
 
 
 # --------------------------------------------------------------------------
