@@ -1191,8 +1191,9 @@ static void bc_vir3(Orc *o, int nb, Reg *rg) {
                 int bi = reg_box_index(rg, i, j, k);
                 int it = rg->image[bi], jt = rg->jmage[bi], kt = rg->kmage[bi];
                 int is = i, js = j, ks = k;
-                if (SA_BC(o)) {
-                    /* parallel.f90:2775-2792 (Sub2.f90:262-278 in place): the
+                if (SA_BC(o) && (!same || o->prm.nvis == 1)) {
+                    /* parallel.f90:2775-2792 (Sub2.f90:262-278 in place, only
+                     * with nvis = 1 there, Sub2.f90:224-228): the
                      * first ghost takes the partner's vist and qke, the face
                      * point the mean of that ghost and its interior neighbour */
                     size_t g = IX(b, i + rg->s_lr3d[0], j + rg->s_lr3d[1], k + rg->s_lr3d[2]);
