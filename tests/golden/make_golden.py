@@ -8,7 +8,9 @@ seeded synthetic cases: a regression pin for the oracle and a fixed target
 for the CUDA path, not a pin against the reference.  Each fixture holds,
 after `nsteps` full steps: the residual RMS of every step, per block and
 variable the sum and the L2 norm of the interior primitive field, and the
-values at 64 seeded interior points per block.
+values at 64 seeded interior points per block (for the SA runs also qke and
+vist).  `python tests/golden/make_golden.py NAME ...` writes only the named
+fixtures.
 """
 import os
 import sys
@@ -26,6 +28,20 @@ GOLDEN = {
     "vortex_roe41": (lambda: cases.vortex_case(ni=33, nj=17, nk=9, nscheme=41, nflux=3), 3),
 }
 PRIM = ("r", "u", "v", "w", "p")
+
+# Spalart-Allmaras runs: the model set up (timedt_turb, kmaxlim) and a seeded
+# non-uniform qke, then whole steps with the model coupled to the mean flow
+SA_GOLDEN = {
+    "small_plate_sa": (lambda: cases.small_plate_case(), 3, 1.0, 0.0),
+}
+
+
+def sa_prepare(obj, case, timedt_turb, kmaxlim):
+    """Set up the model on an oracle or a CUDA context and seed qke."""
+    obj.sa_setup(timedt_turb, kmaxlim)
+    rng = np.random.default_rng(21)
+    for nb, (ni, nj, nk) in enumerate(case.dims, start=1):
+        obj.set("qke", nb, 0.1 * (1.0 + 20.0 * rng.random((nk + 6, nj + 6, ni + 6))))
 
 
 def sample_points(dims, nb, n=64):
@@ -46,10 +62,34 @@ def summarize(get, case, hist):
     return out
 
 
-def main():
+def summarize_sa(get, case, hist):
+    out = summarize(get, case, hist)
+    for nb, d in enumerate(case.dims, start=1):
+        pts = sample_points(d, nb)
+        for name in ("qke", "vist"):
+            a = cases.interior(get(name, nb), d)
+            out[f"b{nb}_{name}_sum"] = np.array([a.sum()])
+            out[f"b{nb}_{name}_l2"] = np.array([np.sqrt((a * a).sum())])
+            out[f"b{nb}_{name}_pts"] = a[pts[:, 0], pts[:, 1], pts[:, 2]].copy()
+    return out
+
+
+def main(names=None):
     from oracle.pyoracle import Oracle, build
     build()
+    for name, (make, nsteps, tt, km) in SA_GOLDEN.items():
+        if names and name not in names:
+            continue
+        case = make()
+        o = Oracle(case)
+        sa_prepare(o, case, tt, km)
+        hist = o.step(nsteps)
+        np.savez(os.path.join(HERE, name + ".npz"), nsteps=np.array([nsteps]), **summarize_sa(o.get, case, hist))
+        o.close()
+        print("wrote", name)
     for name, (make, nsteps) in GOLDEN.items():
+        if names and name not in names:
+            continue
         case = make()
         o = Oracle(case)
         hist = o.step(nsteps)
@@ -59,4 +99,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

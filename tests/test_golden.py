@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from tests.golden.make_golden import GOLDEN, summarize
+from tests.golden.make_golden import GOLDEN, SA_GOLDEN, sa_prepare, summarize, summarize_sa
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TOL_ORACLE = 1e-12
@@ -59,3 +59,13 @@ def test_cuda_path_reproduces_golden(name):
     hist = g.step(nsteps)
     check(summarize(g.get, case, hist), load(name), TOL_GPU)
     g.close()
+
+
+@pytest.mark.parametrize("name", list(SA_GOLDEN))
+def test_oracle_reproduces_sa_golden(oracle_lib, name):
+    make, nsteps, tt, km = SA_GOLDEN[name]
+    case = make()
+    o = oracle_lib.Oracle(case)
+    sa_prepare(o, case, tt, km)
+    hist = o.step(nsteps)
+    check(summarize_sa(o.get, case, hist), load(name), TOL_ORACLE)
