@@ -19,7 +19,8 @@ def header_functions():
     return sorted(set(re.findall(r"\b(wcns_[a-z0-9_]+)\s*\(", text)))
 
 
-@pytest.mark.parametrize("make", [cases.plate_case, cases.small_plate_case, cases.vortex_case])
+@pytest.mark.parametrize("make", [cases.plate_case, cases.small_plate_case, cases.vortex_case,
+                                  cases.channel_case, cases.small_channel_case])
 def test_bc_file_roundtrip(tmp_path, make):
     case = make()
     path = tmp_path / "bc.inp"
@@ -27,6 +28,30 @@ def test_bc_file_roundtrip(tmp_path, make):
     dims, regions = cases.read_bc_file(str(path))
     assert [tuple(d) for d in dims] == [tuple(d) for d in case.dims]
     np.testing.assert_array_equal(regions, case.regions)
+
+
+def test_channel_workload():
+    """The 24-block SA channel: about 4 M points, every face of every block
+    covered by exactly one region, walls on both channel walls."""
+    case = cases.channel_case()
+    assert case.nblocks == 24
+    assert 3.8e6 < case.npoints < 4.3e6
+    assert case.sa == {"timedt_turb": 10.0, "kmaxlim": 30000.0}
+    for nb, (ni, nj, nk) in enumerate(case.dims, start=1):
+        faces = {}
+        for r in case.regions[case.regions[:, 0] == nb]:
+            rng = [(abs(r[1 + 2 * d]), abs(r[2 + 2 * d])) for d in range(3)]
+            d = [q for q in range(3) if rng[q][0] == rng[q][1] and (ni, nj, nk)[q] > 1][0]
+            key = (d, rng[d][0])
+            assert key not in faces
+            assert all(sorted(rng[q]) == [1, (ni, nj, nk)[q]] for q in range(3) if q != d)
+            faces[key] = int(r[7])
+        assert len(faces) == 6
+    assert sorted(set(case.regions[:, 7])) == [-1, 2, 3, 4]
+    # the bump lifts the lower wall at mid-length only
+    lower = [nb for nb in range(1, 25) if any((case.regions[:, 0] == nb) & (case.regions[:, 7] == 2) & (case.regions[:, 3] == 1) & (case.regions[:, 4] == 1))]
+    ymin = min(float(case.xyz[nb - 1][1][:, 0, :].max()) for nb in lower)
+    assert 0.0 < ymin <= 0.05 + 1e-12
 
 
 def test_plate_workload_size():
@@ -43,7 +68,7 @@ def _face_points(xyz, rng):
     return pts[np.lexsort(np.round(pts, 10).T[::-1])]
 
 
-@pytest.mark.parametrize("make", [cases.plate_case, cases.small_plate_case])
+@pytest.mark.parametrize("make", [cases.plate_case, cases.small_plate_case, cases.small_channel_case])
 def test_plate_interfaces_coincide(make):
     """Every one-to-one interface of the plate joins coincident points."""
     case = make()

@@ -144,6 +144,7 @@ SA_BC_CASES = {
     "plate_small": lambda: cases.small_plate_case(),
     "plate_small_sym2d": lambda: cases.small_plate_case(nk=4),
     "supersonic_box": lambda: supersonic_box_case(),
+    "channel_small": lambda: cases.small_channel_case(),
 }
 
 
@@ -221,6 +222,25 @@ def test_oracle_sa_boundary_rules(oracle_lib, name):
     assert min(checked.values()) >= 4, checked
     if name == "plate_small":
         assert ff_sides == {True, False}  # both far-field branches seen
+
+
+def test_oracle_sa_channel_steps(oracle_lib):
+    """The 24-block SA channel (reduced size) runs through the oracle: SA set
+    up with the case's settings, the model's boundary rules on, whole steps;
+    the flow stays finite and the eddy viscosity grows from its free-stream
+    value near the walls."""
+    case = cases.small_channel_case()
+    o = oracle_lib.Oracle(case)
+    o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
+    o.sa_boundary_rules(True)
+    v0 = o.get("vist", 1).copy()
+    hist = o.step(3)
+    assert np.all(np.isfinite(hist))
+    for nb in range(1, len(o.dims) + 1):
+        d = o.dims[nb - 1]
+        for n in ("r", "u", "p", "qke", "vist"):
+            assert np.all(np.isfinite(interior(o.get(n, nb), d)))
+    assert not np.array_equal(o.get("vist", 1), v0)
 
 
 # --------------------------------------------------------------------------

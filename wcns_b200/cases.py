@@ -61,6 +61,9 @@ class Case:
     prim: list = field(default_factory=list)  # [(r,u,v,w,p,t)] ghosted per block
     nsteps: int = 100
     description: str = ""
+    # Spalart-Allmaras settings ($step timedt_turb, $turbulence kmaxlim) for
+    # nlamtur=1, nameturb='SA' runs; None for laminar/Euler cases
+    sa: dict | None = None
 
     @property
     def npoints(self) -> int:
@@ -357,4 +360,108 @@ def small_plate_case(**kw) -> Case:
     return plate_case(**args)
 
 
-CASES = {"vortex": vortex_case, "plate": plate_case, "small_plate": small_plate_case}
+# ----------------------------------------------------------------------------
+# Config 3: turbulent channel with a Gaussian bump, 24 blocks (SA model)
+# ----------------------------------------------------------------------------
+
+def _uneven_splits(n, m, rng, spread=0.25):
+    """m contiguous ranges of the global indices 0..n-1 that share their end
+    points (point-matched interfaces), of seeded uneven length."""
+    base = (n - 1) / m
+    cuts = [0]
+    for b in range(1, m):
+        c = int(round(b * base + rng.uniform(-spread, spread) * base))
+        cuts.append(min(max(c, cuts[-1] + 4), n - 1 - 4 * (m - b)))
+    cuts.append(n - 1)
+    return [(cuts[b], cuts[b + 1]) for b in range(m)]
+
+
+def _tanh_both(n, first):
+    """n points on [0,1] clustered symmetrically at both ends, first spacing
+    about `first`."""
+    eta = np.linspace(-1.0, 1.0, n)
+    lo, hi = 1e-6, 30.0
+    for _ in range(200):
+        beta = 0.5 * (lo + hi)
+        y = 0.5 * (1.0 + np.tanh(beta * eta) / math.tanh(beta))
+        if y[1] - y[0] > first:
+            lo = beta
+        else:
+            hi = beta
+    beta = 0.5 * (lo + hi)
+    return 0.5 * (1.0 + np.tanh(beta * eta) / math.tanh(beta))
+
+
+def channel_case(ni=385, nj=129, nk=81, bx=6, by=2, bz=2, length=6.0, span=1.0, bump=0.05, first=2.0e-6,
+                 nscheme=41, nflux=3, seed=0, nsteps=200) -> Case:
+    """Turbulent channel of height H = 1 with a Gaussian bump of height
+    `bump`*H on the lower wall at mid-length, Re_H = 5e6, Mach 0.6, for the
+    Spalart-Allmaras model (nlamtur=1, nameturb='SA', ncmpcor=0; timedt_turb
+    and kmaxlim as in the reference's param.dat template, 10 and 30000).
+
+    A global ni x nj x nk grid (x along the channel, y across it with tanh
+    clustering at both walls, z spanwise) is cut into bx*by*bz blocks at
+    seeded uneven positions, joined by point-matched one-to-one interfaces.
+    Adiabatic viscous walls (bctype 2) at y = wall and y = H, far field (4) at
+    the inlet and outlet, symmetry (3) on the spanwise faces.  The full size
+    (24 blocks) holds about 4.1 M points."""
+    prm = Params(moo=0.6, reynolds=5.0e6, tref=288.15, twall=-1.0, nvis=1, nscheme=nscheme, nflux=nflux,
+                 cfl=2.0, timedt_rate=1.1, efix=0.1, csrv=1.0)
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0.0, length, ni)
+    eta = _tanh_both(nj, first)
+    zs = np.linspace(0.0, span, nk)
+    sx, sy, sz = _uneven_splits(ni, bx, rng), _uneven_splits(nj, by, rng), _uneven_splits(nk, bz, rng)
+    sigma = 0.1 * length
+    dims, xyz, ids = [], [], {}
+    for iz in range(bz):
+        for iy in range(by):
+            for ix in range(bx):
+                (i0, i1), (j0, j1), (k0, k1) = sx[ix], sy[iy], sz[iz]
+                z, e, x = np.meshgrid(zs[k0:k1 + 1], eta[j0:j1 + 1], xs[i0:i1 + 1], indexing="ij")
+                yw = bump * np.exp(-((x - 0.5 * length) / sigma) ** 2)
+                y = yw + e * (1.0 - yw)
+                dims.append((i1 - i0 + 1, j1 - j0 + 1, k1 - k0 + 1))
+                xyz.append((np.ascontiguousarray(x), np.ascontiguousarray(y), np.ascontiguousarray(z)))
+                ids[(ix, iy, iz)] = len(dims)
+    rl = _RegionList()
+    for (ix, iy, iz), nb in ids.items():
+        d = dims[nb - 1]
+        if ix == 0:
+            rl.add(nb, _face(d, "i-"), 4)
+        else:
+            nbt = ids[(ix - 1, iy, iz)]
+            rl.connect(nb, _face(d, "i-"), nbt, _face(dims[nbt - 1], "i+"))
+        if ix == bx - 1:
+            rl.add(nb, _face(d, "i+"), 4)
+        if iy == 0:
+            rl.add(nb, _face(d, "j-"), 2)
+        else:
+            nbt = ids[(ix, iy - 1, iz)]
+            rl.connect(nb, _face(d, "j-"), nbt, _face(dims[nbt - 1], "j+"))
+        if iy == by - 1:
+            rl.add(nb, _face(d, "j+"), 2)
+        if iz == 0:
+            rl.add(nb, _face(d, "k-"), 3)
+        else:
+            nbt = ids[(ix, iy, iz - 1)]
+            rl.connect(nb, _face(d, "k-"), nbt, _face(dims[nbt - 1], "k+"))
+        if iz == bz - 1:
+            rl.add(nb, _face(d, "k+"), 3)
+    regions = rl.array()
+    prim = [tuple(freestream_prim(prm, d)) for d in dims]
+    npts = sum(a * b * c for a, b, c in dims)
+    return Case("channel", prm, dims, xyz, regions, prim, nsteps,
+                f"SA channel with bump, {len(dims)} blocks, {npts} points",
+                sa={"timedt_turb": 10.0, "kmaxlim": 30000.0})
+
+
+def small_channel_case(**kw) -> Case:
+    """The channel topology (24 blocks) at reduced sizes (for CPU-speed tests)."""
+    args = dict(ni=49, nj=25, nk=13, first=1.0e-3, nsteps=10)
+    args.update(kw)
+    return channel_case(**args)
+
+
+CASES = {"vortex": vortex_case, "plate": plate_case, "small_plate": small_plate_case,
+         "channel": channel_case, "small_channel": small_channel_case}
