@@ -1,24 +1,35 @@
-"""Benchmark: laminar 8-block flat plate (228,888 points), FP64, WCNS-E-5
-(nscheme 41) + Roe + viscous + LU-SGS, one time step of the reference's loop
-(Main.f90:85-109) per timed step.
+"""Benchmark: the SA turbulent channel with a Gaussian wall bump (24 blocks of
+seeded uneven sizes, 4,157,400 points, Re_H 5e6, Mach 0.6), FP64, WCNS-E-5
+(nscheme 41) + Roe + viscous + Spalart-Allmaras + LU-SGS, one time step of
+the reference's loop (Main.f90:85-109) per timed step.  `--case plate` runs
+the laminar 8-block flat plate (228,888 points) instead.
 
 Prints one JSON line.  Metric: Mcell-steps/s = points x steps / seconds.
-  value  -- device-timed: CUDA events around each step's graph replay on the
-            library's stream, inputs resident in HBM; L2 flushed between timed
-            steps (256 MiB write, outside the timed region).
-  e2e    -- the public C ABI with host buffers: per step the prim state of
-            every block is copied in from pinned host memory
-            (wcns_set_prim_all, ghosted layout), the step runs (wcns_step),
-            and the resulting interior state (wcns_get_flow, flow-file
-            layout) and the residual (wcns_residual) are copied back.
+  value  -- device-timed: CUDA events on the library's stream around K graph
+            replays (one replay = one whole step), inputs resident in HBM.
+            The channel's resident fields (about 11 GB) are far larger than
+            L2, so steps run back to back; a workload smaller than 4x L2 is
+            timed step by step with a 256 MiB L2 flush between steps (outside
+            the timed region).
+  phases -- one extra step enqueued phase by phase with CUDA events between
+            the phases (wcns_profile_step), outside the timed region: device
+            ms and share of every phase, the LU-SGS sweeps separately.
+  e2e    -- the public C ABI with host buffers: per step the interior state
+            of every block (r, u, v, w, p and, with the SA model, qke) is
+            copied in from pinned host memory (wcns_set_interior, flow-file
+            layout), the step runs (wcns_step), the same fields are copied
+            back (wcns_get_interior) and the residual read (wcns_residual).
   --impl reference -- the CPU restatement of the reference path (the oracle;
-            the Fortran reference cannot be built here) on all host cores.
+            the Fortran reference cannot be built here) on all host cores,
+            same workload and config.
 N>1 (torchrun): every rank runs its own replica of the case (weak scaling);
 timing is the max over ranks.
 """
 from __future__ import annotations
 
 import argparse
+import glob
+import hashlib
 import json
 import os
 import statistics
@@ -32,9 +43,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# algorithmic bytes per point-step (FP64 words x 8): RHS 20, LU-SGS L 25,
-# U 25, GS-L 30, GS-U 30, update+residual 15 words (1,160 B per point-step)
-WORDS = {"rhs": 20, "lhs": 110, "update": 15, "step": 145}
+L2_BYTES = 126 * 1024 * 1024
+# algorithmic FP64 words per point-step: each globally dependent phase reads
+# its inputs once and writes its outputs once.  Laminar: RHS 20, LU-SGS L 25,
+# U 25, GS-L 30, GS-U 30, update + residual 15 = 145 (1,160 B).  The SA
+# model adds qke/vist to the RHS, its own RHS, two scalar sweeps, the update
+# and the wall distance: 195 words (1,560 B).
+WORDS = {"laminar": 145, "sa": 195}
+PHASE_WORDS = {"sweep_lusgs_l": 25, "sweep_lusgs_u": 25, "sweep_gs_pr_l": 30, "sweep_gs_pr_u": 30}
 
 
 def parse():
@@ -43,7 +59,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--case", default="plate")
+    ap.add_argument("--case", default="channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
     return ap.parse_args()
@@ -93,7 +109,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -137,40 +153,115 @@ def load_peak():
         return 6650.0, "fallback"
 
 
-def load_step_traffic(npoints):
-    """DRAM bytes (read + write) of one time step, summed over the step's
-    kernels from an ncu capture of the plate workload, scaled per point;
-    None when no capture summary is present."""
-    path = os.path.join(ROOT, "profiles", "plate_step_dram.md")
+def sources_digest():
+    """SHA-256 over the CUDA sources, to tie a DRAM-traffic capture to the
+    kernels it was taken from."""
+    h = hashlib.sha256()
+    for p in sorted(glob.glob(os.path.join(ROOT, "wcns_b200", "csrc", "*"))):
+        with open(p, "rb") as f:
+            h.update(os.path.basename(p).encode())
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def load_step_traffic(case_name, npoints):
+    """DRAM bytes (read + write) of one time step, from the ncu summary of
+    this workload under profiles/ (per point-step, scaled by the points).
+    The summary records the digest of the CUDA sources it was captured with;
+    when the sources have changed since, the figure is stale and None is
+    returned with the reason."""
+    path = os.path.join(ROOT, "profiles", f"{case_name}_step_dram.md")
+    per, digest = None, None
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_point_step:"):
-                return int(float(line.split(":")[1]) * npoints)
+                per = float(line.split(":")[1])
+            if line.startswith("sources_digest:"):
+                digest = line.split(":")[1].strip()
     except OSError:
-        pass
-    return None
+        return None, f"no capture summary {os.path.relpath(path, ROOT)}"
+    if per is None:
+        return None, "capture summary without a per-point figure"
+    src = os.path.relpath(path, ROOT)
+    if digest != sources_digest():
+        return None, f"{src} was captured from other kernel sources (digest {digest})"
+    return int(per * npoints), f"{src} (ncu dram__bytes_read.sum + dram__bytes_write.sum over one step's launches)"
 
 
 def make_case(name):
     from wcns_b200 import cases
-    if name == "plate":
-        return cases.plate_case()
-    if name == "vortex":
-        return cases.vortex_case()
     return cases.CASES[name]()
 
 
-def cpu_reference_rate(case, steps, threads=None, target_s=None):
-    """Oracle (CPU restatement) throughput on `steps` full steps of `case`
-    after one untimed step; with `target_s`, the number of steps is chosen
-    from the untimed step so that the timed sample lasts about that long."""
+def sa_prepare(obj, case):
+    """Set up the SA model on a CUDA context when the workload has it (the
+    reference's nlamtur=1, nameturb='SA')."""
+    if case.sa:
+        obj.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
+
+
+def sa_prepare_oracle(o, case):
+    """The same on the oracle, whose brute-force wall distance would take
+    minutes on the full channel: the distance comes from a k-d tree of the
+    wall points instead (set-up work, outside every timed region)."""
+    if not case.sa:
+        return
+    import numpy as np
+    from scipy.spatial import cKDTree
+    o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"], distance=False)
+    wall = []
+    for r in case.regions:
+        if int(r[7]) not in (2, 20, 21):
+            continue
+        x, y, z = case.xyz[int(r[0]) - 1]
+        lo = [min(abs(r[1 + 2 * d]), abs(r[2 + 2 * d])) - 1 for d in range(3)]
+        hi = [max(abs(r[1 + 2 * d]), abs(r[2 + 2 * d])) for d in range(3)]
+        sl = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+        wall.append(np.stack([x[sl].ravel(), y[sl].ravel(), z[sl].ravel()], axis=1))
+    if not wall:
+        return
+    tree = cKDTree(np.concatenate(wall))
+    for nb, (x, y, z) in enumerate(case.xyz, start=1):
+        ni, nj, nk = case.dims[nb - 1]
+        d, _ = tree.query(np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1))
+        full = np.zeros((nk + 6, nj + 6, ni + 6))
+        full[3:3 + nk, 3:3 + nj, 3:3 + ni] = d.reshape(nk, nj, ni) + 1.0e-38
+        o.set("dist", nb, full)
+
+
+def config_of(case, world):
+    resident = case_resident_bytes(case)
+    return {"workload": f"{case.name}: {case.description}", "points": case.npoints, "blocks": case.nblocks,
+            "nscheme": case.params.nscheme, "nflux": case.params.nflux, "nvis": case.params.nvis,
+            "turbulence": "SA" if case.sa else "none", "mach": case.params.moo, "reynolds": case.params.reynolds,
+            "l2": ("inputs larger than L2: %.1f GB of fields resident, steps back to back" % (resident / 1e9))
+            if resident > 4 * L2_BYTES else "256 MiB L2 flush between timed steps",
+            "parallelism": f"replicas x{world}"}
+
+
+def case_resident_bytes(case):
+    """Device bytes the step touches: the field pool (48 doubles per ghosted
+    point), the sweep arrays and the SA fields."""
+    ghosted = sum((a + 6) * (b + 6) * (c + 6) for a, b, c in case.dims)
+    plane = sum((a + b + c - 2) * b * c for a, b, c in case.dims)
+    return 8 * (48 * ghosted + 99 * plane + (8 * ghosted if case.sa else 0))
+
+
+def cpu_reference_rate(case, steps, threads=None, target_s=None, max_s=None):
+    """Oracle (CPU restatement) throughput on full steps of `case` after one
+    untimed step.  With `target_s` the number of steps is chosen from the
+    untimed step so that the timed sample lasts about that long; `max_s`
+    caps the sample of a fixed step count."""
     from oracle.pyoracle import Oracle
     o = Oracle(case, nthreads=threads or os.cpu_count())
+    sa_prepare_oracle(o, case)
     t0 = time.perf_counter()
     o.step(1)
     one = time.perf_counter() - t0
     if target_s:
         steps = int(min(200, max(steps, round(target_s / max(one, 1e-3)))))
+    if max_s:
+        steps = int(max(1, min(steps, max_s // max(one, 1e-3))))
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
@@ -183,19 +274,30 @@ def run_reference(args, rank, world):
         return
     case = make_case(args.case)
     cores = os.cpu_count()
-    # each step is one full step of the workload on all host cores
-    rate, dt, _ = cpu_reference_rate(case, max(1, args.steps), cores)
+    # each timed step is one full step of the workload on all host cores;
+    # the count is capped so that the sample stays within about 100 s
+    rate, dt, n = cpu_reference_rate(case, max(1, args.steps), cores, max_s=100.0)
     line = {
         "metric": METRIC, "value": round(rate, 4), "unit": "Mcell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(1e3 * dt / max(1, args.steps), 3), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * dt / n, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": f"{case.name}: {case.description}", "points": case.npoints, "blocks": case.nblocks},
+        "config": config_of(case, world),
         "cpu_baseline": {"value": round(rate, 4), "unit": "Mcell-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} full steps of the workload after 1 untimed step (OpenMP over blocks/lines)"},
+                         "sample": f"{n} full steps of the workload after 1 untimed step ({dt:.1f} s; OpenMP over "
+                                   f"blocks and lines; the oracle restatement, the Fortran cannot be built here)"},
         "e2e": {"value": round(rate, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def profile_phases(g, reps=3):
+    """Median device ms of every phase over `reps` profiled steps."""
+    runs = [g.profile_step() for _ in range(reps)]
+    out = []
+    for q, (name, _) in enumerate(runs[0]):
+        out.append((name, statistics.median(r[q][1] for r in runs)))
+    return out
 
 
 def run_b200(args, rank, world):
@@ -206,62 +308,84 @@ def run_b200(args, rank, world):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     case = make_case(args.case)
     g = Wcns(case)
+    sa_prepare(g, case)
     stream = torch.cuda.ExternalStream(g.stream)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    big = case_resident_bytes(case) > 4 * L2_BYTES
+    flush = None if big else torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     # warm-up
     g.step(args.warmup, history=False)
     dist_barrier(world)
     torch.cuda.synchronize()
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
-    evs = []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-        g.step_async(1)
+    if big:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step_async(args.steps)
         e1.record(stream)
-        evs.append((e0, e1))
-    g.sync()
-    torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in evs)
+        g.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+    else:
+        evs = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            g.step_async(1)
+            b.record(stream)
+            evs.append((a, b))
+        g.sync()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
     clk = clocks.stop()
     dist_barrier(world)
     ms = dist_max(ms, world)
     total_points = case.npoints * world
     value = total_points * args.steps / (ms / 1e3) / 1e6
+    step_ms = ms / args.steps
 
     # Roofline of the step program: one graph replay = one step of the whole
-    # path.  Algorithmic bytes = the compulsory traffic of one point-step
-    # (WORDS["step"] FP64 words: each globally dependent phase reads its
-    # inputs once and writes its outputs once) x points; duration = the
-    # CUDA-event time of the timed steps above.
+    # path.  Algorithmic bytes = the compulsory traffic of one point-step x
+    # points; duration = the CUDA-event time per step above.
     peak, peak_kind = load_peak()
-    step_bytes = case.npoints * WORDS["step"] * 8
-    achieved = step_bytes / (ms / args.steps / 1e3) / 1e9
-    traffic = load_step_traffic(case.npoints)
+    words = WORDS["sa" if case.sa else "laminar"]
+    step_bytes = case.npoints * words * 8
+    achieved = step_bytes / (step_ms / 1e3) / 1e9
+    traffic, traffic_src = load_step_traffic(case.name, case.npoints)
 
-    # end-to-end through the C ABI with pinned host buffers
-    pinned = []
-    for nb, d in enumerate(case.dims, start=1):
-        ni, nj, nk = d
-        bufs = [torch.empty((nk + 6, nj + 6, ni + 6), dtype=torch.float64, pin_memory=True).numpy() for _ in range(6)]
-        for f, name in enumerate(("r", "u", "v", "w", "p", "t")):
-            bufs[f][...] = g.get(name, nb)
-        pinned.append(bufs)
-    # results: the interior state of every block in the flow-file layout
-    outs = [[torch.empty((nk, nj, ni), dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
+    # per-phase device times (one extra profiled step each, outside the timed region)
+    phases = profile_phases(g)
+    tot = sum(t for _, t in phases)
+    ph = []
+    for name, t in phases:
+        e = {"phase": name, "ms": round(t, 4), "share": round(t / tot, 4) if tot else None}
+        if name in PHASE_WORDS and t > 0:
+            gbs = case.npoints * PHASE_WORDS[name] * 8 / (t / 1e3) / 1e9
+            e.update(gbs=round(gbs, 1), frac=round(gbs / peak, 4))
+        ph.append(e)
+    dom = max(ph, key=lambda e: e["ms"])
+    sweeps = [e for e in ph if e["phase"].startswith("sweep_")]
+
+    # end-to-end through the C ABI with pinned host buffers: interior state in
+    # and out in the flow-file layout
+    names = ["r", "u", "v", "w", "p"] + (["qke"] if case.sa else [])
+    pin = [[torch.empty((nk, nj, ni), dtype=torch.float64, pin_memory=True).numpy() for _ in names]
+           for ni, nj, nk in case.dims]
+    g.get_interior(names, pin)
+    outs = [[torch.empty((nk, nj, ni), dtype=torch.float64, pin_memory=True).numpy() for _ in names]
             for ni, nj, nk in case.dims]
-    h2d = sum(6 * a[0].size * 8 for a in pinned)
-    d2h = sum(5 * a[0].size * 8 for a in outs) + 8 * (2 * case.nblocks + 1)
+    h2d = sum(a.size * 8 for arrs in pin for a in arrs)
+    d2h = sum(a.size * 8 for arrs in outs for a in arrs) + 8 * (2 * case.nblocks + 1)
     dist_barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        g.set_prim_all(pinned)
+        g.set_interior(names, pin)
         g.step(1, history=False)
-        g.get_flow(outs)
+        g.get_interior(names, outs)
         g.residual_curve()
     e2e_s = time.perf_counter() - t0
     e2e_s = dist_max(e2e_s, world)
@@ -270,7 +394,7 @@ def run_b200(args, rank, world):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, dt, n = cpu_reference_rate(case, 3, os.cpu_count(), target_s=10.0)
+            rate, dt, n = cpu_reference_rate(case, 3, os.cpu_count(), target_s=15.0)
             cpu = {"value": round(rate, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"{n} full steps of the workload after 1 untimed step ({dt:.1f} s, OpenMP)"}
         except Exception as e:  # the baseline is reported, never required
@@ -279,19 +403,21 @@ def run_b200(args, rank, world):
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"{case.name}: {case.description}", "points": case.npoints,
-                       "blocks": case.nblocks, "nscheme": case.params.nscheme, "nflux": case.params.nflux,
-                       "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"},
+            "config": config_of(case, world),
             "e2e": {"value": round(e2e, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "kernel": "one time step (CUDA graph of the whole path)",
                          "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": int(step_bytes), "launch_ms": round(ms / args.steps, 4),
-                         "traffic": traffic},
+                         "algorithmic_bytes_per_launch": int(step_bytes), "bytes_per_point_step": words * 8,
+                         "launch_ms": round(step_ms, 4), "traffic": traffic, "traffic_source": traffic_src,
+                         "dominant_phase": dom["phase"],
+                         "sweeps": {"share": round(sum(e["share"] for e in sweeps), 4),
+                                    "ms": round(sum(e["ms"] for e in sweeps), 4)}},
+            "phases": ph,
             "gpu_launches": g.launches_per_step() * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -6,7 +6,7 @@
  * The reference exposes this path as argument-less Fortran subroutines that
  * act on module globals and are called from its time loop (Main.f90:79-127).
  * Each entry point below replaces one of those calls; a Fortran driver binds
- * them with iso_c_binding (see INTEGRATION.md).  All functions return 0 on
+ * them with iso_c_binding.  All functions return 0 on
  * success and a nonzero WcnsStatus otherwise; wcns_last_error() gives the
  * message.  No exception crosses this boundary.  One host thread drives one
  * context; all device work of a context is ordered on the context's stream.
@@ -24,8 +24,9 @@ extern "C" {
 
 /* The param.dat namelist values the path reads ($inflow, $step, $flowtype,
  * $technic; read_parameter, PreProcess.f90:80-159).  Supported: nvis 0 or 1
- * (laminar), nscheme 4, 41 or 42, nflux 1 (Steger-Warming), 2 (Van Leer) or
- * 3 (Roe); anything else is rejected with WCNS_ERR_UNSUPPORTED. */
+ * (viscous; laminar, or turbulent once wcns_sa_setup has run), nscheme 4, 41
+ * or 42, nflux 1 (Steger-Warming), 2 (Van Leer) or 3 (Roe); anything else is
+ * rejected with WCNS_ERR_UNSUPPORTED. */
 typedef struct WcnsParams {
     double moo, attack, sideslip, reynolds, tref, twall;
     double cfl, timedt_rate, efix, csrv;
@@ -89,12 +90,23 @@ int wcns_get_prim_all(WcnsContext *ctx, double *const *prim);
  * t skipping T of that block.  One synchronisation. */
 int wcns_get_flow(WcnsContext *ctx, double *const *flow);
 int wcns_set_field(WcnsContext *ctx, int field, int nb, const double *in);
+/* Interior points of any of the fields above for every block, in the
+ * flow-file layout (ni*nj*nk doubles per array, i fastest, no ghost
+ * layers), with one synchronisation: ptrs holds nfields pointers per block
+ * in block order (ptrs[nfields*(nb-1) + q] is field fields[q] of block nb); a
+ * NULL pointer skips that array.  wcns_set_interior leaves every ghost point
+ * as it was on the device (the next wcns_boundary_all refills the ghost
+ * layers the path reads): the restart read of a flow file (init_nstart1,
+ * Sub2.f90:367-405) without its ghost frame. */
+int wcns_set_interior(WcnsContext *ctx, int nfields, const int *fields, const double *const *ptrs);
+int wcns_get_interior(WcnsContext *ctx, int nfields, const int *fields, double *const *ptrs);
 
 /* Per-step drop-ins, in the reference's call order (Main.f90:85-109). */
 int wcns_boundary_all(WcnsContext *ctx);        /* exchange_bc + boundary_all (Main.f90:85-87) */
 int wcns_initial_q_dq_c_t(WcnsContext *ctx);    /* initial_q_dq_c_t (sub_tgh.f90:1-32) */
 int wcns_timestep(WcnsContext *ctx);            /* timestep_tgh (sub_tgh.f90:1270-1348) */
-int wcns_rhs_vis(WcnsContext *ctx);             /* r_h_s_vis (RHS.f90:2-30), laminar */
+int wcns_rhs_vis(WcnsContext *ctx);             /* r_h_s_vis (RHS.f90:2-30); with the SA model
+                                                   set up it first runs the model step, see below */
 int wcns_communicate_dq(WcnsContext *ctx);      /* communicate_dq_npp (parallel.f90:3020-3058) */
 int wcns_rhs_invis(WcnsContext *ctx);           /* r_h_s_invis (RHS.f90:35-72) */
 int wcns_lhs(WcnsContext *ctx);                 /* l_h_s_tgh (LHS.f90:1-34) */
@@ -111,12 +123,24 @@ int wcns_residual(WcnsContext *ctx, double *res_per_block, double *resmax_per_bl
  * wcns_create), sets qke and vist to their free-stream values over the
  * points -1..n+1 (init_SA, turblence.f90:2701-2733) and keeps timedt_turb
  * ($step) and kmaxlim ($turbulence; <= 1e-15 for no clamp).  Needs nvis 1.
- * wcns_turbulence: one model step on every block (source, diffusion,
- * spectral radius, convection, scalar LU-SGS, update of qke at the
- * interior points 2..n-1, vist at 1..n, kmaxlim clamp at 0..n), reading the
- * current prim, visl and dtdt.  The ghost values of qke are the caller's
- * (set with wcns_set_field): the model's boundary conditions and the use of
- * vist in the mean-flow viscous flux are not part of this library. */
+ * Once the model is set up:
+ *   - wcns_rhs_vis runs the model step first, as r_h_s_vis calls
+ *     turbulence(nb) (RHS.f90:22), and the viscous flux then uses visl+vist
+ *     and visl*cp/prl + vist*cp/prt; wcns_timestep adds the eddy viscosity to
+ *     the viscous spectral radii (spectvist, LHS.f90:141-241).  A driver that
+ *     calls wcns_rhs_vis must not also call wcns_turbulence in the same step,
+ *     or the model advances twice.
+ *   - wcns_boundary_all also applies the model's one-layer qke/vist boundary
+ *     rules inside each BC routine (interface copies and face means,
+ *     parallel.f90:2775-2792 and Sub2.f90:262-278; far field
+ *     BC_farfield_turbulence_tgh, sub_tgh.f90:713-787; inflow, outflow,
+ *     wall and symmetry, BC.f90:269,416,627-640,686-721,1280,1301).
+ *   - wcns_step includes all of this.
+ * wcns_turbulence: one model step on every block on its own (source,
+ * diffusion, spectral radius, convection, scalar LU-SGS, update of qke at
+ * the interior points 2..n-1, vist at 1..n, kmaxlim clamp at 0..n), reading
+ * the current prim, visl and dtdt: for drivers that sequence the model
+ * themselves. */
 int wcns_sa_setup(WcnsContext *ctx, const double *const *xyz, double timedt_turb, double kmaxlim);
 int wcns_turbulence(WcnsContext *ctx);
 
@@ -139,6 +163,13 @@ int wcns_sync(WcnsContext *ctx);
 void *wcns_stream(WcnsContext *ctx);
 /* Number of kernel launches one step issues. */
 int wcns_launches_per_step(WcnsContext *ctx);
+/* One whole step (it advances the state like wcns_step(ctx, 1, NULL)),
+ * enqueued phase by phase instead of from the graph, with a CUDA event after
+ * each phase: ms[q] receives the device time of phase q and names[q] its
+ * name (a static string: boundary_all, the SA model's parts, rhs_vis,
+ * rhs_invis, the four LU-SGS sweeps, ...), *nphases the count (at most cap).
+ * For profiling; the graph replay of wcns_step is what production runs. */
+int wcns_profile_step(WcnsContext *ctx, int cap, double *ms, const char **names, int *nphases);
 /* Number of points shared by more than two blocks (multi-point sets). */
 int wcns_n_multipoints(WcnsContext *ctx);
 
@@ -156,10 +187,14 @@ int wcns_n_multipoints(WcnsContext *ctx);
  * 150 KB, held by every GPU that loads the library until the process exits),
  * which limits nblocks to WCNS_NOALLOC_MAX_BLOCKS; larger counts are
  * rejected with WCNS_ERR_ARGUMENT.  The first call on a device looks up that
- * array's device address, so make it before any stream capture.  Every call
- * on a device shares the array: calls that overlap on the GPU (other host
- * threads, other streams) race and must be serialised by the caller.  The
- * call returns after the results are on the host. */
+ * array's device address and keeps it per device ordinal, which assumes one
+ * CUDA context per device in the process (the runtime's primary context).
+ * Every call synchronises its stream and copies the results to the host, so
+ * it must not be called while its stream (or the legacy default stream) is
+ * being captured into a CUDA graph.  Every call on a device shares the
+ * array: calls that overlap on the GPU (other host threads, other streams)
+ * race and must be serialised by the caller.  The call returns after the
+ * results are on the host. */
 #define WCNS_NOALLOC_MAX_BLOCKS 256
 int wcns_residual_noalloc(int nblocks, const int *dims, const double *const *fields, double *res_per_block,
                           double *resmax_per_block, double *rms, void *stream);

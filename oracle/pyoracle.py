@@ -147,7 +147,9 @@ class Oracle:
         lib().orc_sa_boundary_rules.argtypes = [C.c_void_p, C.c_int]
         assert lib().orc_sa_boundary_rules(self.h, 1 if on else 0) == 0
 
-    def sa_setup(self, timedt_turb=1.0, kmaxlim=0.0):
+    def sa_setup(self, timedt_turb=1.0, kmaxlim=0.0, distance=True):
+        """init_SA and the model's settings; with distance=False the wall
+        distance is not computed (set field "dist" afterwards)."""
         L = lib()
-        L.orc_sa_setup.argtypes = [C.c_void_p, C.c_double, C.c_double]
-        assert L.orc_sa_setup(self.h, timedt_turb, kmaxlim) == 0
+        L.orc_sa_setup_ex.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+        assert L.orc_sa_setup_ex(self.h, timedt_turb, kmaxlim, 1 if distance else 0) == 0

@@ -2629,7 +2629,9 @@ static void sa_init(Blk *b, double cv13) {
             }
 }
 
-int orc_sa_setup(void *h, double timedt_turb, double kmaxlim) {
+int orc_sa_setup(void *h, double timedt_turb, double kmaxlim) { return orc_sa_setup_ex(h, timedt_turb, kmaxlim, 1); }
+
+int orc_sa_setup_ex(void *h, double timedt_turb, double kmaxlim, int with_distance) {
     Orc *o = h;
     const double cv13 = pow(SA_CV1, 3.0);
     for (int nb = 1; nb <= o->nb; nb++) {
@@ -2647,8 +2649,9 @@ int orc_sa_setup(void *h, double timedt_turb, double kmaxlim) {
     }
     o->timedt_turb = timedt_turb;
     o->kmaxlim = kmaxlim;
+    if (!o->sa) o->sa_bc = 1; /* the reference always applies the model's BC rules (nlamtur >= 0) */
     o->sa = 1;
-    sa_wall_distance(o);
+    if (with_distance) sa_wall_distance(o);
     return 0;
 }
 
@@ -2921,12 +2924,14 @@ static void sa_block(const Orc *o, Blk *b) {
                 }
 }
 
-/* turbulence(nb) for every block (RHS.f90:22 inside r_h_s_vis) */
+/* on/off switch of the model's qke/vist BC rules (on from orc_sa_setup);
+ * the known-answer test turns them off to see that they are the only change */
 int orc_sa_boundary_rules(void *h, int on) {
     ((Orc *)h)->sa_bc = on ? 1 : 0;
     return 0;
 }
 
+/* turbulence(nb) for every block (RHS.f90:22 inside r_h_s_vis) */
 int orc_turbulence(void *h) {
     Orc *o = h;
     if (!o->sa) { set_err("orc_turbulence: orc_sa_setup was not called"); return 1; }

@@ -63,10 +63,15 @@ int orc_forces(void *h, const double *ref, double *out);
  * timedt_turb and kmaxlim; fields 28, 29, 30 (qke, vist, wall distance) are
  * then readable and writable, and orc_turbulence runs the model step. */
 int orc_sa_setup(void *h, double timedt_turb, double kmaxlim);
+/* with_distance 0: as orc_sa_setup but without the brute-force wall distance
+ * (O(points x wall points)); the caller sets field 30 itself.  For timing
+ * runs on large grids, where the distance is set-up work outside the step. */
+int orc_sa_setup_ex(void *h, double timedt_turb, double kmaxlim, int with_distance);
 int orc_turbulence(void *h);
 /* on != 0: orc_boundary_all also applies the model's one-layer qke/vist
  * rules of every BC routine (BC_*_turbulence, the interface copies and face
- * means).  Off by default: the CUDA path does not apply them yet. */
+ * means).  orc_sa_setup turns them on, as the reference always applies them
+ * when a turbulence model runs; off is for the known-answer test only. */
 int orc_sa_boundary_rules(void *h, int on);
 
 /* line-operator hooks used by the known-answer tests */

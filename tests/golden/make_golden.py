@@ -31,8 +31,10 @@ PRIM = ("r", "u", "v", "w", "p")
 
 # Spalart-Allmaras runs: the model set up (timedt_turb, kmaxlim) and a seeded
 # non-uniform qke, then whole steps with the model coupled to the mean flow
+# and its qke/vist boundary rules applied in boundary_all
 SA_GOLDEN = {
     "small_plate_sa": (lambda: cases.small_plate_case(), 3, 1.0, 0.0),
+    "small_channel_sa": (lambda: cases.small_channel_case(), 3, 10.0, 30000.0),
 }
 
 

@@ -114,3 +114,43 @@ def perturbed(case, amp=0.05, seed=5):
         cases.interior(r, d)[...] = cases.interior(r, d) * (1.0 + bump)
         cases.interior(p, d)[...] = cases.interior(p, d) * (1.0 + 1.4 * bump)
     return case
+
+
+GAMMA = 1.4
+
+
+def conserved(get, nb, dims):
+    """Conserved variables (rho, rho u, rho v, rho w, e) at the interior
+    points of block nb from its primitive fields (prim_to_q, Sub1.f90:106)."""
+    r, u, v, w, p = (interior(get(n, nb), dims) for n in ("r", "u", "v", "w", "p"))
+    return [r, r * u, r * v, r * w, p / (GAMMA - 1.0) + 0.5 * r * (u * u + v * v + w * w)]
+
+
+def compare_conserved(gpu, orc, blocks=None):
+    """max |gpu - oracle| of each conserved variable over all blocks, relative
+    to the variable's maximum magnitude over the case; the three momentum
+    components share the scale of the momentum magnitude (a component that
+    vanishes by symmetry has no scale of its own)."""
+    nbs = blocks or range(1, len(orc.dims) + 1)
+    num = [0.0] * 5
+    den = [0.0] * 5
+    mom = 0.0
+    for nb in nbs:
+        d = orc.dims[nb - 1]
+        a, b = conserved(gpu.get, nb, d), conserved(orc.get, nb, d)
+        for m in range(5):
+            num[m] = max(num[m], float(np.max(np.abs(a[m] - b[m]))))
+            den[m] = max(den[m], float(np.max(np.abs(b[m]))))
+        mom = max(mom, float(np.max(np.sqrt(b[1] ** 2 + b[2] ** 2 + b[3] ** 2))))
+    names = ("rho", "rho_u", "rho_v", "rho_w", "e")
+    return {n: (num[m] / (mom if m in (1, 2, 3) else den[m]) if num[m] else 0.0) for m, n in enumerate(names)}
+
+
+def residual_block_errors(gpu, orc):
+    """Relative difference of the per-block residual L2 (residual_curve), its
+    maximum and the RMS over all blocks."""
+    rg, ro = gpu.residual_curve(), orc.residual()
+    res = float(np.max(np.abs(rg[0] - ro[0]) / np.abs(ro[0])))
+    rmax = float(np.max(np.abs(rg[1] - ro[1]) / np.abs(ro[1])))
+    rms = abs(rg[2] - ro[2]) / abs(ro[2])
+    return {"res_l2_per_block": res, "resmax_per_block": rmax, "rms": rms}

@@ -69,3 +69,16 @@ def test_oracle_reproduces_sa_golden(oracle_lib, name):
     sa_prepare(o, case, tt, km)
     hist = o.step(nsteps)
     check(summarize_sa(o.get, case, hist), load(name), TOL_ORACLE)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(SA_GOLDEN))
+def test_cuda_path_reproduces_sa_golden(name):
+    from wcns_b200.solver import Wcns
+    make, nsteps, tt, km = SA_GOLDEN[name]
+    case = make()
+    g = Wcns(case)
+    sa_prepare(g, case, tt, km)
+    hist = g.step(nsteps)
+    check(summarize_sa(g.get, case, hist), load(name), TOL_GPU)
+    g.close()

@@ -167,7 +167,8 @@ def test_oracle_sa_boundary_rules(oracle_lib, name):
         v = 1e-6 * (1.0 + rng.random(q.shape))
         o.set("qke", nb, q); o.set("vist", nb, v)
         pre_q[nb], pre_v[nb] = q, v
-    # off by default: boundary_all leaves qke alone
+    # switched off, boundary_all leaves qke alone: the rules are the only change
+    o.sa_boundary_rules(False)
     o.phase("boundary_all")
     assert all(np.array_equal(o.get("qke", nb), pre_q[nb]) for nb in pre_q)
     for nb in pre_q:
@@ -232,7 +233,6 @@ def test_oracle_sa_channel_steps(oracle_lib):
     case = cases.small_channel_case()
     o = oracle_lib.Oracle(case)
     o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
-    o.sa_boundary_rules(True)
     v0 = o.get("vist", 1).copy()
     hist = o.step(3)
     assert np.all(np.isfinite(hist))
@@ -335,3 +335,73 @@ def test_sa_errors():
     with pytest.raises(WcnsError) as ei:
         e.sa_setup()
     assert ei.value.code == 5
+
+
+# the model's qke/vist boundary rules on the device: cases that between them
+# reach every rule (channel: cross-block interfaces, adiabatic walls, far
+# field both ways, symmetry; viscous vortex: self-connected interfaces in
+# place; viscous Mach-2 box: supersonic inflow and outflow)
+SA_RULE_CASES = {
+    "channel_small": lambda: cases.small_channel_case(),
+    "plate_small": lambda: cases.small_plate_case(),
+    "plate_small_sym2d": lambda: cases.small_plate_case(nk=4),
+    "vortex_viscous": SA_CASES["vortex_viscous"],
+    "supersonic_box_vis": lambda: with_params(supersonic_box_case(), nvis=1),
+}
+
+PHASES = [("boundary_all", "boundary_all"), ("initial_q_dq_c_t", "initial_q_dq_c_t"), ("timestep_tgh", "timestep"),
+          ("r_h_s_vis", "rhs_vis"), ("communicate_dq_npp", "communicate_dq"), ("r_h_s_invis", "rhs_invis"),
+          ("communicate_dq_npp", "communicate_dq"), ("l_h_s_tgh", "lhs"), ("communicate_pv_npp", "communicate_pv")]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(SA_RULE_CASES))
+def test_sa_boundary_rules_parity(name):
+    """boundary_all with the model set up: qke and vist at every point of
+    the ghosted box (face points and first ghosts included) equal the
+    oracle's after the rules, bitwise (copies, negations and means of equal
+    inputs; the far-field branch is picked by the sign of a contravariant
+    velocity, which agrees here); then a whole step phase by phase, each
+    quantity within 1e-12 of its scale."""
+    case = SA_RULE_CASES[name]()
+    tt, km = (case.sa["timedt_turb"], case.sa["kmaxlim"]) if case.sa else (1.5, 0.0)
+    g, o = _pair(case)
+    g.sa_setup(tt, km); o.sa_setup(tt, km)
+    rng = np.random.default_rng(17)
+    for nb in range(1, len(o.dims) + 1):
+        q = MUOO * (1.0 + 5.0 * rng.random(o.get("qke", nb).shape))
+        v = 1e-5 * (1.0 + rng.random(q.shape))
+        g.set("qke", nb, q); o.set("qke", nb, q)
+        g.set("vist", nb, v); o.set("vist", nb, v)
+    g.boundary_all(); o.phase("boundary_all")
+    e = compare_fields(g, o, ["qke", "vist"], region="all")
+    assert max(e.values()) == 0.0, e
+    e = compare_fields(g, o, ["r", "u", "v", "w", "p"], region="all")
+    assert max(e.values()) <= TOL, e
+    for gp, op in PHASES[1:]:
+        getattr(g, gp)(); o.phase(op)
+        names = {"initial_q_dq_c_t": ["t"], "timestep_tgh": ["dtdt", "sra", "srva", "srvb", "srvc"],
+                 "r_h_s_vis": ["qke", "vist", "dq1", "dq2", "dq3", "dq4", "dq5"],
+                 "communicate_dq_npp": ["dq1", "dq2", "dq3", "dq4", "dq5"],
+                 "r_h_s_invis": ["dq1", "dq2", "dq3", "dq4", "dq5"],
+                 "l_h_s_tgh": ["r", "u", "v", "w", "p"], "communicate_pv_npp": ["r", "u", "v", "w", "p", "t"]}[gp]
+        e = compare_fields(g, o, names, region="all" if gp == "r_h_s_vis" else "interior")
+        assert max(e.values()) <= TOL, (gp, e)
+    rg, ro = g.residual_curve(), o.residual()
+    np.testing.assert_allclose(rg[0], ro[0], rtol=TOL, atol=0)
+    np.testing.assert_allclose(rg[2], ro[2], rtol=TOL, atol=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["channel_small", "vortex_viscous", "supersonic_box_vis"])
+def test_sa_rules_graph_steps(name):
+    """Whole steps through the step graph with the model and its boundary
+    rules: residual history, conserved-variable fields and qke/vist."""
+    case = SA_RULE_CASES[name]()
+    tt, km = (case.sa["timedt_turb"], case.sa["kmaxlim"]) if case.sa else (1.5, 0.0)
+    g, o = _pair(case)
+    g.sa_setup(tt, km); o.sa_setup(tt, km)
+    hg, ho = g.step(5), o.step(5)
+    np.testing.assert_allclose(hg, ho, rtol=1e-12, atol=0)
+    e = compare_fields(g, o, ["r", "u", "v", "w", "p", "qke", "vist"], region="all")
+    assert max(e.values()) <= 1e-12, e

@@ -31,6 +31,9 @@ SIGNATURES = {
     "wcns_get_prim_all": (C.c_int, [_VP, C.POINTER(C.c_void_p)]),
     "wcns_get_flow": (C.c_int, [_VP, C.POINTER(C.c_void_p)]),
     "wcns_set_field": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "wcns_set_interior": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p)]),
+    "wcns_get_interior": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p)]),
+    "wcns_profile_step": (C.c_int, [_VP, C.c_int, _VP, C.POINTER(C.c_char_p), C.POINTER(C.c_int)]),
     "wcns_boundary_all": (C.c_int, [_VP]),
     "wcns_initial_q_dq_c_t": (C.c_int, [_VP]),
     "wcns_timestep": (C.c_int, [_VP]),

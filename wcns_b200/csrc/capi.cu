@@ -265,18 +265,30 @@ static int build_tables(WcnsContext *c) {
     // physical regions in bcindex order, dq-zero points
     std::vector<DevRegion> regs;
     std::vector<int> first(nbk + 1, 0);
-    std::vector<long long> zero;
+    std::vector<long long> zero, sa_src;
     for (int b = 0; b < nbk; b++) {
         first[b] = (int)regs.size();
         for (int r : c->blk[b].bcindex) {
             const HReg &R = c->blk[b].regs[r];
-            if (R.bctype < 0) continue;
             DevRegion d{};
             d.blk = b;
-            d.bctype = R.bctype;
+            d.bctype = R.bctype < 0 ? -1 : R.bctype;
             for (int m = 0; m < 3; m++) { d.s_st[m] = R.s_st[m]; d.s_ed[m] = R.s_ed[m]; d.s_lr3d[m] = R.s_lr3d[m]; }
             d.s_nd = R.s_nd;
             d.s_lr = R.s_lr;
+            if (R.bctype < 0) {
+                // the SA interface rule reads the partner's first interior
+                // point behind the image point (parallel.f90:2763-2766)
+                d.same = R.nbt == b + 1 ? 1 : 0;
+                d.sa_first = (long long)sa_src.size();
+                for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                    for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                        for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                            int bx = R.box(i, j, k);
+                            sa_src.push_back(c->gi(R.nbt, R.img[0][bx] - R.t_lr3d[0], R.img[1][bx] - R.t_lr3d[1],
+                                                   R.img[2][bx] - R.t_lr3d[2]));
+                        }
+            }
             regs.push_back(d);
         }
         for (const HReg &R : c->blk[b].regs) {
@@ -289,6 +301,12 @@ static int build_tables(WcnsContext *c) {
     first[nbk] = (int)regs.size();
     L.regions = c->up(regs);
     L.reg_first = c->up(first);
+    L.nsa_if = (long long)sa_src.size();
+    L.sa_if_src = c->up(sa_src);
+    if (L.nsa_if) {
+        CK(cudaMalloc(&L.sa_if_snap, sizeof(double) * 2 * (size_t)L.nsa_if));
+        c->owned.push_back(L.sa_if_snap);
+    }
     L.nzero = (long long)zero.size();
     L.zero_pts = c->up(zero);
     // interface averaging: snapshot slots, pairs per region (region order)
@@ -892,6 +910,52 @@ extern "C" int wcns_get_flow(WcnsContext *c, double *const *flow) {
     return 0;
 }
 
+// Interior points of any public fields of every block, in the flow-file
+// layout (i = 1..ni fastest, then j, then k, no ghost layers), both ways:
+// ptrs[nfields * b + q] is field fields[q] of block b+1; a null pointer skips
+// that array.  One strided copy per array, spread over the context's three
+// streams, one synchronisation.  Writing leaves every ghost point as it was:
+// boundary_all refills the ghost layers the path reads.
+static int interior_copy(WcnsContext *c, int nfields, const int *fields, double *const *ptrs, bool to_device) {
+    const char *fn = to_device ? "wcns_set_interior" : "wcns_get_interior";
+    if (!c || nfields < 1 || !fields || !ptrs) { set_err(std::string(fn) + ": invalid argument"); return WCNS_ERR_ARGUMENT; }
+    for (int q = 0; q < nfields; q++)
+        if (!field_base(c, fields[q])) { set_err(std::string(fn) + ": unsupported field " + std::to_string(fields[q])); return WCNS_ERR_UNSUPPORTED; }
+    CK(cudaEventRecord(c->L.ev_fork, c->stream));
+    cudaStream_t st[3] = {c->stream, c->L.side[0], c->L.side[1]};
+    for (int q = 1; q < 3; q++) CK(cudaStreamWaitEvent(st[q], c->L.ev_fork, 0));
+    int e = 0;
+    const int nbk = (int)c->blk.size();
+    for (int b = 0; b < nbk; b++) {
+        const DevBlock &d = c->blk[b].d;
+        for (int q = 0; q < nfields; q++) {
+            double *host = ptrs[(size_t)nfields * b + q];
+            if (!host) continue;
+            cudaPitchedPtr dev = make_cudaPitchedPtr(field_base(c, fields[q]) + d.off, sizeof(double) * d.gx, d.gx, d.gy);
+            cudaPitchedPtr hp = make_cudaPitchedPtr(host, sizeof(double) * d.ni, d.ni, d.nj);
+            cudaMemcpy3DParms cp = {};
+            cp.srcPtr = to_device ? hp : dev;
+            cp.dstPtr = to_device ? dev : hp;
+            // the ghosted box (-2:n+3) starts 3 points before the interior in each direction
+            (to_device ? cp.dstPos : cp.srcPos) = make_cudaPos(sizeof(double) * 3, 3, 3);
+            cp.extent = make_cudaExtent(sizeof(double) * d.ni, d.nj, d.nk);
+            cp.kind = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+            CK(cudaMemcpy3DAsync(&cp, st[e % 3]));
+            e++;
+        }
+    }
+    for (int q = 0; q < 3; q++) CK(cudaStreamSynchronize(st[q]));
+    return 0;
+}
+
+extern "C" int wcns_set_interior(WcnsContext *c, int nfields, const int *fields, const double *const *ptrs) {
+    return interior_copy(c, nfields, fields, const_cast<double *const *>(ptrs), true);
+}
+
+extern "C" int wcns_get_interior(WcnsContext *c, int nfields, const int *fields, double *const *ptrs) {
+    return interior_copy(c, nfields, fields, ptrs, false);
+}
+
 extern "C" int wcns_set_field(WcnsContext *c, int field, int nb, const double *in) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;
@@ -1055,26 +1119,71 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     LaunchCtx &L = c->L;
     int n = 0;
     launch_boundary(L); n += 2;
+    prof_mark(L, "boundary_all");
     launch_init_timestep(L); n += 1;
+    prof_mark(L, "initial_q_dq_c_t+timestep");
     if (c->P.nvis == 1) {
         if (c->sa_pool) { launch_turbulence(L); n += 4; }
         launch_node_derivatives(L); n += 1;
         launch_rhs_dirs(L, true);
         for (int d = 0; d < 3; d++) n += L.vis[d].ngroups ? 1 : 0;
         n += (L.vis[1].ngroups || L.vis[2].ngroups) ? 1 : 0;
+        prof_mark(L, "rhs_vis");
         launch_communicate(L, 0); n += L.nsnap ? 2 : 0;
+        prof_mark(L, "communicate_dq");
     }
     launch_rhs_dirs(L, false);
     for (int d = 0; d < 3; d++) n += L.inv[d].ngroups ? 1 : 0;
     n += (L.inv[1].ngroups || L.inv[2].ngroups) ? 1 : 0;
+    prof_mark(L, "rhs_invis");
     launch_communicate(L, 0); n += L.nsnap ? 2 : 0;
+    prof_mark(L, "communicate_dq");
     launch_lhs(L); n += 6 + (L.nzero ? 2 : 0);  // prep, four sweeps, plane-major dq to the fields
     launch_update(L); n += 2;
+    prof_mark(L, "update");
     launch_communicate(L, 1); n += L.nsnap ? 2 : 0;
+    prof_mark(L, "communicate_pv");
     launch_residual(L, rms_slot); n += 2;
+    prof_mark(L, "residual");
     c->launches = n;
     CK(cudaGetLastError());
     return 0;
+}
+
+// One whole step enqueued phase by phase (not from the graph) with an event
+// after each phase; ms[q] is the device time of phase q, names[q] its name
+// (static strings), *nphases their count (at most cap).  The step advances
+// the state like wcns_step(c, 1, NULL).
+extern "C" int wcns_profile_step(WcnsContext *c, int cap, double *ms, const char **names, int *nphases) {
+    if (!c || cap < 1 || !ms || !names || !nphases) { set_err("wcns_profile_step: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    std::vector<cudaEvent_t> ev(cap + 1, nullptr);
+    std::vector<const char *> nm(cap, nullptr);
+    int rc = 0;
+    for (auto &e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) { set_err("wcns_profile_step: event creation failed"); rc = WCNS_ERR_CUDA; }
+    if (!rc) {
+        ProfMarks pm;
+        pm.cap = cap;
+        pm.ev = ev.data() + 1;
+        pm.name = nm.data();
+        cudaEventRecord(ev[0], c->stream);
+        c->L.prof = &pm;
+        rc = enqueue_step(c, nullptr);
+        c->L.prof = nullptr;
+        if (!rc) rc = check_errors(c);
+        if (!rc) {
+            for (int q = 0; q < pm.n; q++) {
+                float t = 0.0f;
+                cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+                ms[q] = t;
+                names[q] = nm[q];
+            }
+            *nphases = pm.n;
+        }
+    }
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    return rc;
 }
 
 static int build_graph(WcnsContext *c) {

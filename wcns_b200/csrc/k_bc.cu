@@ -23,12 +23,26 @@ namespace cg = cooperative_groups;
 
 namespace wcns {
 
-__global__ void k_ghost_copy(DevFields F, const GhostCopy *__restrict__ list, long long n) {
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+constexpr double SA_MUOO_BC = 1.0e-1;  // muoo, the model's free-stream value (inflow_turbulence, turblence.f90:3174)
+
+// With the SA model set up (qke != null) the same launch also takes the
+// start-of-pass snapshot of qke and vist at the interface rule's source
+// points (the exchange buffer qpvpack, parallel.f90:2775-2792), before the
+// BC walk writes any face point.
+__global__ void k_ghost_copy(DevFields F, const GhostCopy *__restrict__ list, long long n, const double *__restrict__ qke,
+                             const long long *__restrict__ sa_src, double *__restrict__ sa_snap, long long nsa) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
         GhostCopy g = list[e];
 #pragma unroll
         for (int f = 0; f < 5; f++) F.f[F_R + f][g.dst] = F.f[F_R + f][g.src];
     }
+    if (qke)
+        for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nsa; e += stride) {
+            const long long s = sa_src[e];
+            sa_snap[2 * e] = qke[s];
+            sa_snap[2 * e + 1] = F.f[F_VIST][s];
+        }
 }
 
 __device__ __forceinline__ void set5(DevFields &F, long long id, double r, double u, double v, double w, double p) {
@@ -55,16 +69,37 @@ __device__ __forceinline__ void getnxyz(const DevFields &F, long long id, int is
 // One cluster of BC_CLUSTER CTAs per block: the points of a region are
 // spread over the whole cluster, and a cluster barrier (release/acquire at
 // cluster scope, covering the global-memory writes) separates regions.
+// With the SA model set up (qke != null), each BC routine also applies the
+// model's one-layer qke rules where the reference calls them inside it (F:
+// face point, G = F + s_lr3d the first ghost, T = F - s_lr3d):
+//   interface  G <- partner (snapshot, or in place for a self-connection),
+//              F <- (G + T)/2, for vist too (parallel.f90:2775-2792,
+//              Sub2.f90:262-278)
+//   far field  F, G <- muoo where the boundary state flows in, else T
+//              (BC_farfield_turbulence_tgh, sub_tgh.f90:713-787; BC.f90:570)
+//   inflow     F, G <- muoo (BC.f90:627-640)
+//   outflow    F, G <- T (BC.f90:686-721)
+//   wall       G <- -T, F <- (T + G)/2 (BC_wall_turbulence, BC.f90:1280,
+//              BC_face_dif_turbulence 1301, turblence.f90:2238-2300)
+//   symmetry   G <- T (clamped to the block in 2-D), F <- (T + G)/2
+//              (BC_symmetry_turbulence BC.f90:269,416; dif_average 2002)
+// Interface regions come first in a block's list (set_bc_index), so a point
+// that two regions share keeps the later region's value, as in the
+// reference's sequence.
 __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                      const DevRegion *__restrict__ regions,
-                                                     const int *__restrict__ reg_first) {
+                                                     const int *__restrict__ reg_first, double *__restrict__ qke,
+                                                     const long long *__restrict__ sa_src,
+                                                     const double *__restrict__ sa_snap) {
     cg::cluster_group cluster = cg::this_cluster();
     const int bi = blockIdx.x / BC_CLUSTER;
     const int t0 = (int)cluster.block_rank() * blockDim.x + threadIdx.x, tstride = BC_CLUSTER * blockDim.x;
     const DevBlock B = blocks[bi];
     const int r0 = reg_first[bi], r1 = reg_first[bi + 1];
+    double *vist = F.f[F_VIST];
     for (int r = r0; r < r1; r++) {
         const DevRegion R = regions[r];
+        if (R.bctype < 0 && !qke) continue;  // uniform over the cluster: no barrier is skipped by a part of it
         const int *L = R.s_lr3d;
         const int e0 = R.s_ed[0] - R.s_st[0] + 1, e1 = R.s_ed[1] - R.s_st[1] + 1, e2 = R.s_ed[2] - R.s_st[2] + 1;
         const int npts = e0 * e1 * e2;
@@ -127,6 +162,15 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                     rb = P.roo; ub = P.uoo; vb = P.voo; wb = P.woo; pb = P.poo;
                 }
                 set5(F, f, rb, ub, vb, wb, pb);
+                if (qke) {
+                    // contravariant velocity of the boundary state with the
+                    // face point's metrics of the face direction
+                    const int m0 = F_KCX + 3 * (R.s_nd - 1);
+                    double ut = (double)L[R.s_nd - 1] * (F.f[m0][f] * ub + F.f[m0 + 1][f] * vb + F.f[m0 + 2][f] * wb);
+                    double qt = qke[tI];
+                    qke[f] = ut < 0.0 ? SA_MUOO_BC : qt;
+                    qke[f + sL] = ut < 0.0 ? SA_MUOO_BC : qt;
+                }
                 set5(F, f + sL, rb, ub, vb, wb, pb);
                 set5(F, f + 2 * sL, rb, ub, vb, wb, pb);
                 set5(F, f + 3 * sL, -rb, ub, vb, wb, pb);
@@ -134,18 +178,28 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
             }
             case 5: {  // supersonic inflow
                 for (int n = 0; n <= 3; n++) set5(F, f + n * sL, P.roo, P.uoo, P.voo, P.woo, P.poo);
+                if (qke) qke[f] = qke[f + sL] = SA_MUOO_BC;
                 break;
             }
             case 6: {  // supersonic outflow
                 long long tI = f - sL;
                 double rm = rr[tI], um = uu[tI], vm = vv[tI], wm = ww[tI], pm = pp[tI];
                 for (int n = 0; n <= 3; n++) set5(F, f + n * sL, rm, um, vm, wm, pm);
+                if (qke) {
+                    double qt = qke[tI];
+                    qke[f] = qt;
+                    qke[f + sL] = qt;
+                }
                 break;
             }
             case 2: {
                 if (P.nvis == 1) {  // viscous wall
                     long long t1 = f - sL, t2 = f - 2 * sL, t3 = f - 3 * sL;
                     set5(F, f + sL, rr[t1], -uu[t1], -vv[t1], -ww[t1], pp[t1]);
+                    if (qke) {
+                        qke[f + sL] = -qke[t1];
+                        qke[f] = 0.5 * (qke[t1] + qke[f + sL]);
+                    }
                     double pres = (4.0 * pp[t1] - pp[t2]) / 3.0;
                     double tres;
                     if (P.adiabatic) {
@@ -173,6 +227,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                     long long s = f + sL, tI = f - sL;
                     set5(F, f, 0.5 * (rr[s] + rr[tI]), 0.5 * (uu[s] + uu[tI]), 0.5 * (vv[s] + vv[tI]), 0.5 * (ww[s] + ww[tI]),
                          0.5 * (pp[s] + pp[tI]));
+                    if (qke) qke[f] = 0.5 * (qke[tI] + qke[s]);
                 }
                 break;
             }
@@ -183,6 +238,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                     jt = jt < 1 ? 1 : (jt > B.nj ? B.nj : jt);
                     kt = kt < 1 ? 1 : (kt > B.nk ? B.nk : kt);
                     long long tI = gidx(B, it, jt, kt);
+                    if (qke) qke[f + sL] = qke[tI];
                     double rm = rr[tI], um = uu[tI], vm = vv[tI], wm = -ww[tI], pm = pp[tI];
                     set5(F, f + sL, rm, um, vm, wm, pm);
                     set5(F, f + 2 * sL, rm, um, vm, 0.0, pm);
@@ -192,11 +248,24 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                         long long s = f + l * sL, tI = f - l * sL;
                         double s1 = 2.0 * (snx * uu[tI] + sny * vv[tI] + snz * ww[tI]);
                         set5(F, s, rr[tI], uu[tI] - s1 * snx, vv[tI] - s1 * sny, ww[tI] - s1 * snz, pp[tI]);
+                        if (l == 1 && qke) qke[s] = qke[tI];
                     }
                 }
                 long long s = f + sL, tI = f - sL;
                 set5(F, f, 0.5 * (rr[s] + rr[tI]), 0.5 * (uu[s] + uu[tI]), 0.5 * (vv[s] + vv[tI]), 0.5 * (ww[s] + ww[tI]),
                      0.5 * (pp[s] + pp[tI]));
+                if (qke) qke[f] = 0.5 * (qke[tI] + qke[s]);
+                break;
+            }
+            case -1: {  // interface: the SA model's qke/vist copy and face mean
+                const long long e = R.sa_first + t, g = f + sL, tI = f - sL;
+                double pv, pq;
+                if (R.same) { pq = qke[sa_src[e]]; pv = vist[sa_src[e]]; }
+                else { pq = sa_snap[2 * e]; pv = sa_snap[2 * e + 1]; }
+                vist[g] = pv;
+                vist[f] = (vist[g] + vist[tI]) * 0.5;
+                qke[g] = pq;
+                qke[f] = (qke[g] + qke[tI]) * 0.5;
                 break;
             }
             default: break;
@@ -210,10 +279,13 @@ void launch_boundary(const LaunchCtx &c) {
     if (c.nghost > 0) {
         int grid = (int)((c.nghost + 255) / 256);
         if (grid > 148 * 16) grid = 148 * 16;
-        k_ghost_copy<<<grid, 256, 0, c.stream>>>(*c.F, c.ghost, c.nghost);
+        k_ghost_copy<<<grid, 256, 0, c.stream>>>(*c.F, c.ghost, c.nghost, c.SA ? c.SA->qke : nullptr, c.sa_if_src,
+                                                 c.sa_if_snap, c.nsa_if);
     }
+    double *qke = c.SA ? c.SA->qke : nullptr;
     launch_block_clusters(k_bc_physical, c.nblocks, 512, c.stream, *c.P, *c.F, (const DevBlock *)c.blocks,
-                          (const DevRegion *)c.regions, (const int *)c.reg_first);
+                          (const DevRegion *)c.regions, (const int *)c.reg_first, qke, (const long long *)c.sa_if_src,
+                          (const double *)c.sa_if_snap);
 }
 
 }  // namespace wcns

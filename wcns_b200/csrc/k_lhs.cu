@@ -683,12 +683,18 @@ void launch_lhs(const LaunchCtx &c) {
     if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
     const dim3 pg128((unsigned)((maxp + PREP_THREADS - 1) / PREP_THREADS), c.nblocks);
     k_lhs_prep<<<pg128, PREP_THREADS, 0, c.stream>>>(*c.P, *c.F, *c.PM, c.blocks);
+    prof_mark(c, "lhs_prep");
     launch_sweep<0>(c);
+    prof_mark(c, "sweep_lusgs_l");
     launch_sweep<1>(c);
+    prof_mark(c, "sweep_lusgs_u");
     launch_sweep<2>(c);
+    prof_mark(c, "sweep_gs_pr_l");
     launch_sweep<3>(c);
+    prof_mark(c, "sweep_gs_pr_u");
     k_pm_to_std<<<pg, 256, 0, c.stream>>>(*c.F, *c.PM, c.blocks);
     if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
+    prof_mark(c, "lhs_store");
 }
 
 }  // namespace wcns

@@ -19,10 +19,16 @@ struct DirTable {
 };
 
 // One boundary region as the device sees it (bcindex order within a block).
+// Interface regions (bctype -1) are in the list too: the BC walk applies the
+// SA model's qke/vist copies there when the model is set up, and skips them
+// otherwise.  sa_first: the region's first entry in the interface source
+// list (LaunchCtx::sa_if_src); same: 1 for a block connected to itself.
 struct DevRegion {
     int blk, bctype;
     int s_st[3], s_ed[3];
     int s_nd, s_lr, s_lr3d[3];
+    int same;
+    long long sa_first;
 };
 
 // interface ghost copy: ghost (dst) <- partner interior (src)
@@ -60,7 +66,16 @@ struct SaParams {
     double reynolds, re, ki2, cv13, cw36, onesix, cw1, timedt_turb, kmaxlim;
 };
 
+// Phase marks for wcns_profile_step: an event recorded on the context stream
+// after each phase of a step enqueued outside the graph (null: no marks).
+struct ProfMarks {
+    int n = 0, cap = 0;
+    cudaEvent_t *ev = nullptr;
+    const char **name = nullptr;
+};
+
 struct LaunchCtx {
+    ProfMarks *prof = nullptr;
     cudaStream_t stream = 0;
     long long total = 0;               // points of the field pool (stride of a field)
     // the three directions of a residual run concurrently: directions 1 and 2
@@ -78,9 +93,15 @@ struct LaunchCtx {
     // boundary conditions
     GhostCopy *ghost = nullptr;
     long long nghost = 0;
-    DevRegion *regions = nullptr;  // physical regions, grouped per block in bcindex order
+    DevRegion *regions = nullptr;  // all regions, grouped per block in bcindex order (-1 first)
     int *reg_first = nullptr;      // per block: first region index (nblocks+1 entries), device
     int max_regions_per_block = 0;
+    // SA interface rule: per interface face point (region order, i fastest)
+    // the partner's point whose qke/vist go to the first ghost, and a
+    // start-of-pass snapshot of those two values (2 per point)
+    long long *sa_if_src = nullptr;
+    double *sa_if_snap = nullptr;
+    long long nsa_if = 0;
     // dq-zero list (points on physical faces)
     long long *zero_pts = nullptr;
     long long nzero = 0;
@@ -119,6 +140,12 @@ struct LaunchCtx {
 };
 
 constexpr int BAD_CAP = 512;
+
+inline void prof_mark(const LaunchCtx &c, const char *name) {
+    if (!c.prof || c.prof->n >= c.prof->cap) return;
+    cudaEventRecord(c.prof->ev[c.prof->n], c.stream);
+    c.prof->name[c.prof->n++] = name;
+}
 
 // CTAs per block for the kernels that walk a block's BC or interface
 // regions in order (one cluster per block, cluster barrier between regions)

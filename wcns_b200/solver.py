@@ -162,6 +162,48 @@ class Wcns:
                 raise ValueError(f"block {nb}: array has the wrong shape, dtype or layout")
         return [a.ctypes.data for a in arrs]
 
+    def _interior_ptrs(self, names, arrays):
+        if len(arrays) != len(self.dims):
+            raise ValueError("one list of arrays per block")
+        fields = (C.c_int * len(names))(*[FID[n] for n in names])
+        ptrs = []
+        for (ni, nj, nk), arrs in zip(self.dims, arrays):
+            if len(arrs) != len(names):
+                raise ValueError(f"{len(names)} arrays per block")
+            for a in arrs:
+                if a is None:
+                    ptrs.append(None)
+                    continue
+                if a.shape != (nk, nj, ni) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError("interior array has the wrong shape, dtype or layout")
+                ptrs.append(a.ctypes.data)
+        return fields, (C.c_void_p * len(ptrs))(*ptrs)
+
+    def set_interior(self, names, arrays):
+        """Set the interior points (flow-file layout, shape (nk, nj, ni)) of
+        the named fields of every block: arrays[nb-1][q] is field names[q]
+        of block nb (None skips it); ghost points keep their device values."""
+        fields, vec = self._interior_ptrs(names, arrays)
+        _check(_lib.load().wcns_set_interior(self.h, len(names), fields, vec))
+
+    def get_interior(self, names, arrays=None):
+        """Copy the interior points of the named fields of every block into
+        `arrays` (allocated when None); returns them."""
+        if arrays is None:
+            arrays = [[np.empty((nk, nj, ni)) for _ in names] for ni, nj, nk in self.dims]
+        fields, vec = self._interior_ptrs(names, arrays)
+        _check(_lib.load().wcns_get_interior(self.h, len(names), fields, vec))
+        return arrays
+
+    def profile_step(self, cap=64):
+        """One whole step enqueued phase by phase with CUDA events between
+        the phases: list of (phase name, device ms).  Advances the state."""
+        ms = np.zeros(cap)
+        names = (C.c_char_p * cap)()
+        n = C.c_int(0)
+        _check(_lib.load().wcns_profile_step(self.h, cap, ms.ctypes.data, names, C.byref(n)))
+        return [(names[q].decode(), float(ms[q])) for q in range(n.value)]
+
     def set(self, name, nb, arr):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
         _check(_lib.load().wcns_set_field(self.h, FID[name], nb, arr.ctypes.data))
