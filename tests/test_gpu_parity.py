@@ -200,3 +200,29 @@ def test_get_flow_is_the_interior():
     for a, b in zip(five, flow):
         for x, y in zip(a, b[:5]):
             assert np.array_equal(x, y)
+
+
+# the sweeps as one launch per hyperplane (the path of blocks too large for
+# the clustered sweep kernel), asked for on cases that would use the kernel
+PLANE_CASES = ["vortex_roe_41", "plate_small", "plate_small_euler_wall", "supersonic_box_sw4"]
+
+
+@pytest.mark.parametrize("name", PLANE_CASES)
+def test_sweep_by_plane_matches_oracle(name):
+    from oracle.pyoracle import Oracle
+    from wcns_b200.solver import FLAG_SWEEP_BY_PLANE, Wcns
+    case = CASES[name]()
+    g, o = Wcns(case, flags=FLAG_SWEEP_BY_PLANE), Oracle(case)
+    for gp, op in [("boundary_all", "boundary_all"), ("initial_q_dq_c_t", "initial_q_dq_c_t"),
+                   ("timestep_tgh", "timestep")] + ([("r_h_s_vis", "rhs_vis"), ("communicate_dq_npp", "communicate_dq")]
+                                                    if case.params.nvis else []) + \
+                  [("r_h_s_invis", "rhs_invis"), ("communicate_dq_npp", "communicate_dq"), ("l_h_s_tgh", "lhs")]:
+        getattr(g, gp)()
+        o.phase(op)
+    e = compare_fields(g, o, DQ + PRIM)
+    assert max(e.values()) <= TOL_PHASE, e
+    g.communicate_pv_npp(); o.phase("communicate_pv")
+    hg, ho = g.step(5), o.step(5)
+    np.testing.assert_allclose(hg, ho, rtol=1e-12, atol=0)
+    e = compare_prim_scaled(g, o)
+    assert max(e.values()) <= 1e-12, e

@@ -513,7 +513,8 @@ static int build_tables(WcnsContext *c) {
         int cl = 16, fine = 1;
         if (const char *e = getenv("WCNS_SWEEP_CLUSTER")) cl = atoi(e);
         if (const char *e = getenv("WCNS_SWEEP_FINE")) fine = atoi(e);
-        if (setup_sweep(L, cl, fine)) { set_err("a block has too many (j,k) columns for the sweep kernel"); return WCNS_ERR_ARGUMENT; }
+        // blocks whose columns do not fit the clustered kernel sweep plane by plane
+        L.sweep_plane = (c->prm.flags & WCNS_FLAG_SWEEP_BY_PLANE) || setup_sweep(L, cl, fine) ? 1 : 0;
     }
     // residual partials, update bad lists
     L.res_ctas_per_block = 32;
@@ -639,18 +640,6 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     cudaMemset(c->pool, 0, bytes);
     for (int f = 0; f < F_NPOOL; f++) c->F.f[f] = c->pool + (size_t)f * c->total;
     c->F.f[F_VIST] = nullptr;
-    // sweep arrays, plane-major: dq (5 planes of values), the static records
-    // (SR_N per cell) and three dynamic records (DYN_N per cell); the memset
-    // leaves zero the records that no kernel ever writes
-    size_t pmbytes = sizeof(double) * (size_t)(5 + SR_N + 3 * DYN_N) * (size_t)c->total_pm;
-    if (cudaMalloc(&c->pm_pool, pmbytes) != cudaSuccess) { delete c; set_err("device allocation of the sweep arrays failed"); return WCNS_ERR_CUDA; }
-    cudaMemset(c->pm_pool, 0, pmbytes);
-    for (int m = 0; m < 5; m++) c->PM.dq[m] = c->pm_pool + (size_t)m * c->total_pm;
-    c->PM.dq_stride = c->total_pm;
-    c->PM.stat = c->pm_pool + (size_t)5 * c->total_pm;
-    c->PM.dyn = c->PM.stat + (size_t)SR_N * c->total_pm;
-    c->PM.gs[0] = c->PM.dyn + (size_t)DYN_N * c->total_pm;
-    c->PM.gs[1] = c->PM.gs[0] + (size_t)DYN_N * c->total_pm;
     std::vector<DevBlock> hb(nblocks);
     for (int b = 0; b < nblocks; b++) hb[b] = c->blk[b].d;
     LaunchCtx &L = c->L;
@@ -683,6 +672,20 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     }
     rc = build_tables(c);
     if (rc) { delete c; return rc; }
+    if (!L.sweep_plane) {
+        // sweep arrays, plane-major: dq (5 planes of values), the static records
+        // (SR_N per cell) and three dynamic records (DYN_N per cell); the memset
+        // leaves zero the records that no kernel ever writes
+        size_t pmbytes = sizeof(double) * (size_t)(5 + SR_N + 3 * DYN_N) * (size_t)c->total_pm;
+        if (cudaMalloc(&c->pm_pool, pmbytes) != cudaSuccess) { delete c; set_err("device allocation of the sweep arrays failed"); return WCNS_ERR_CUDA; }
+        cudaMemset(c->pm_pool, 0, pmbytes);
+        for (int m = 0; m < 5; m++) c->PM.dq[m] = c->pm_pool + (size_t)m * c->total_pm;
+        c->PM.dq_stride = c->total_pm;
+        c->PM.stat = c->pm_pool + (size_t)5 * c->total_pm;
+        c->PM.dyn = c->PM.stat + (size_t)SR_N * c->total_pm;
+        c->PM.gs[0] = c->PM.dyn + (size_t)DYN_N * c->total_pm;
+        c->PM.gs[1] = c->PM.gs[0] + (size_t)DYN_N * c->total_pm;
+    }
     c->PM.csize = L.sweep_cluster;
     CK(cudaMalloc(&c->d_err, sizeof(int) * ERR_NSLOTS));
     c->owned.push_back(c->d_err);
@@ -1138,7 +1141,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     prof_mark(L, "rhs_invis");
     launch_communicate(L, 0); n += L.nsnap ? 2 : 0;
     prof_mark(L, "communicate_dq");
-    launch_lhs(L); n += 6 + (L.nzero ? 2 : 0);  // prep, four sweeps, plane-major dq to the fields
+    n += launch_lhs(L);
     launch_update(L); n += 2;
     prof_mark(L, "update");
     launch_communicate(L, 1); n += L.nsnap ? 2 : 0;
@@ -1212,6 +1215,11 @@ extern "C" int wcns_sync(WcnsContext *c) {
     return check_errors(c);
 }
 
+// The error slots are read after every step, so that a multi-step call
+// stops after the first step at which the reference would stop
+// (update_limited's bad-point limit, Sub2.f90:781-785; the Roe c^2 check,
+// flux.f90:179-182): the state is that after the failing step, later steps
+// are not run and their rms_history entries are left untouched.
 extern "C" int wcns_step(WcnsContext *c, int nsteps, double *rms_history) {
     if (!c || nsteps < 0) { set_err("wcns_step: invalid argument"); return WCNS_ERR_ARGUMENT; }
     if (int rc = build_graph(c)) return rc;
@@ -1219,7 +1227,25 @@ extern "C" int wcns_step(WcnsContext *c, int nsteps, double *rms_history) {
     for (int s = 0; s < nsteps; s++) {
         CK(cudaGraphLaunch(c->graph, c->stream));
         if (rms_history) CK(cudaMemcpyAsync(rms_history + s, c->L.res_out + 2 * nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (int rc = check_errors(c)) {
+            g_err += " (step " + std::to_string(s + 1) + " of " + std::to_string(nsteps) + " of this call)";
+            return rc;
+        }
     }
+    return 0;
+}
+
+// The LU-SGS sweep's bounded wait on an mbarrier that nothing completes,
+// with a limit of limit_cycles clock cycles: returns what a step returns
+// after a sweep timed out (WCNS_ERR_CUDA and its message), with no other
+// work in flight, and leaves the context usable.
+extern "C" int wcns_selftest_timeout(WcnsContext *c, long long limit_cycles) {
+    if (!c || limit_cycles < 0 || limit_cycles > (1LL << 32)) {
+        set_err("wcns_selftest_timeout: invalid argument (0 <= limit_cycles <= 2^32)");
+        return WCNS_ERR_ARGUMENT;
+    }
+    launch_wait_probe(c->L, limit_cycles);
+    CK(cudaGetLastError());
     return check_errors(c);
 }
 

@@ -589,6 +589,20 @@ __global__ void __launch_bounds__(FINE ? SWEEP_FINE_MAX_THREADS : SWEEP_COARSE_M
     if (timed_out) atomicAdd(&err[ERR_TIMEOUT], 1);
 }
 
+// One thread initialises an mbarrier that nothing arrives at and waits for
+// its first phase with the sweep's bounded wait; the wait gives up after
+// `limit` cycles and the timeout is reported in the error slot the sweeps
+// use.  No copy or remote store is in flight, so giving up is safe.
+__global__ void k_wait_probe(int *err, long long limit) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    if (!mbar_wait(&bar, 0u, limit)) atomicAdd(&err[ERR_TIMEOUT], 1);
+}
+
+void launch_wait_probe(const LaunchCtx &c, long long limit) { k_wait_probe<<<1, 32, 0, c.stream>>>(c.err, limit); }
+
 template <int MODE, bool FINE>
 static void launch_sweep_t(const LaunchCtx &c) {
     cudaLaunchConfig_t cfg = {};
@@ -675,8 +689,17 @@ int setup_sweep(LaunchCtx &c, int cluster, int fine) {
     return -1;
 }
 
-void launch_lhs(const LaunchCtx &c) {
+int launch_lhs(const LaunchCtx &c) {
     const int zg = (int)((c.nzero + 255) / 256);
+    if (c.sweep_plane) {
+        // set_nonconnect_boundary_dq_0, the sweeps plane by plane, again the faces
+        if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
+        prof_mark(c, "lhs_prep");
+        int n = launch_sweeps_by_plane(c);
+        if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
+        prof_mark(c, "lhs_store");
+        return n + (c.nzero > 0 ? 2 : 0);
+    }
     long long maxp = 0;
     for (int b = 0; b < c.nblocks; b++) maxp = std::max(maxp, pm_size(c.hblocks[b]));
     const dim3 pg((unsigned)((maxp + 255) / 256), c.nblocks);
@@ -695,6 +718,7 @@ void launch_lhs(const LaunchCtx &c) {
     k_pm_to_std<<<pg, 256, 0, c.stream>>>(*c.F, *c.PM, c.blocks);
     if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
     prof_mark(c, "lhs_store");
+    return 6 + (c.nzero > 0 ? 2 : 0);  // prep, four sweeps, plane-major dq to the fields
 }
 
 }  // namespace wcns

@@ -58,7 +58,17 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_partial(const NaBlock *__rest
     const long long np = (mi > 0 && mj > 0 && mk > 0) ? (long long)mi * mj * mk : 0;
     double s = 0.0, mx = 0.0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < np; q += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(q % mi) + 2, j = (int)((q / mi) % mj) + 2, k = (int)(q / ((long long)mi * mj)) + 2;
+        int i, j, k;
+        if (q < 0x7fffffffLL) {  // 32-bit divisions where they suffice
+            const int qq = (int)q, r = qq / mi;
+            i = qq - r * mi + 2;
+            j = r % mj + 2;
+            k = r / mj + 2;
+        } else {
+            i = (int)(q % mi) + 2;
+            j = (int)((q / mi) % mj) + 2;
+            k = (int)(q / ((long long)mi * mj)) + 2;
+        }
         const long long id = na_idx(B, i, j, k);
         const double dtime1 = 1.0 / (B.f[5][id] * B.f[6][id]);
 #pragma unroll

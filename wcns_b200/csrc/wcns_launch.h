@@ -125,6 +125,9 @@ struct LaunchCtx {
     double *res_out = nullptr;      // per block: res, resmax; then rms
     // LU-SGS sweeps: CTAs per block cluster, columns per CTA, threads per CTA
     int sweep_cluster = 1, sweep_cpc = 1, sweep_threads = 32, sweep_fine = 0;
+    // 1: the sweeps run as one launch per hyperplane on the field layout
+    // (blocks too large for the clustered kernel, or asked for)
+    int sweep_plane = 0;
     const PmFields *PM = nullptr;  // plane-major sweep arrays
     // wall forces
     DevWall *walls = nullptr;
@@ -184,8 +187,11 @@ void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);
 void launch_init_timestep(const LaunchCtx &c);
 void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
-void launch_lhs(const LaunchCtx &c);
+int launch_lhs(const LaunchCtx &c);  // returns the number of launches
+int launch_sweeps_by_plane(const LaunchCtx &c);
 int setup_sweep(LaunchCtx &c, int cluster, int fine);
+// the sweeps' bounded wait on an mbarrier nothing completes (self-test)
+void launch_wait_probe(const LaunchCtx &c, long long limit);
 void launch_update(const LaunchCtx &c);
 void launch_forces(const LaunchCtx &c, double xref, double yref, double zref);
 void launch_residual(const LaunchCtx &c, double *rms_slot);

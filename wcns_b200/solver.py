@@ -33,19 +33,22 @@ def _check(rc):
         raise WcnsError(rc, _lib.last_error())
 
 
-def params_struct(p) -> _lib.WcnsParams:
+FLAG_SWEEP_BY_PLANE = 1  # WCNS_FLAG_SWEEP_BY_PLANE
+
+
+def params_struct(p, flags=0) -> _lib.WcnsParams:
     return _lib.WcnsParams(p.moo, p.attack, p.sideslip, p.reynolds, p.tref, p.twall, p.cfl, p.timedt_rate, p.efix,
-                           p.csrv, p.nvis, p.nscheme, p.nflux, 0)
+                           p.csrv, p.nvis, p.nscheme, p.nflux, flags)
 
 
 class Wcns:
     """One multi-block case resident on the GPU."""
 
-    def __init__(self, case):
+    def __init__(self, case, flags=0):
         L = _lib.load()
         self.case = case
         self.dims = [tuple(int(v) for v in d) for d in case.dims]
-        self._prm = params_struct(case.params)
+        self._prm = params_struct(case.params, flags)
         dims = (C.c_int * (3 * len(self.dims)))(*[v for d in self.dims for v in d])
         keep, ptrs = [], []
         for xyz in case.xyz:
@@ -275,6 +278,11 @@ class Wcns:
 
     def launches_per_step(self) -> int:
         return int(_lib.load().wcns_launches_per_step(self.h))
+
+    def selftest_timeout(self, limit_cycles=1000):
+        """The sweeps' bounded wait on an mbarrier nothing completes: raises
+        WcnsError (WCNS_ERR_CUDA) as a step does after a sweep timeout."""
+        _check(_lib.load().wcns_selftest_timeout(self.h, limit_cycles))
 
     def n_multipoints(self) -> int:
         return int(_lib.load().wcns_n_multipoints(self.h))
