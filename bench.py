@@ -418,6 +418,7 @@ def run_b200(args, rank, world):
                          "sweeps": {"share": round(sum(e["share"] for e in sweeps), 4),
                                     "ms": round(sum(e["ms"] for e in sweeps), 4)}},
             "phases": ph,
+            "sweep_mode": g.sweep_mode(),
             "gpu_launches": g.launches_per_step() * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,

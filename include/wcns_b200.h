@@ -38,6 +38,12 @@ typedef struct WcnsParams {
  * columns than the clustered sweep kernel holds; the flag asks for it on
  * any case (same results). */
 #define WCNS_FLAG_SWEEP_BY_PLANE 1
+/* Run the LU-SGS sweeps as wide cooperative sweeps: chunks of whole j-rows
+ * of a block per CTA, all CTAs resident, neighbouring chunks coupled through
+ * rings of planes in device memory.  The context picks this by itself for
+ * blocks too large for the clustered sweep kernel; the flag asks for it on
+ * any case that fits (same results). */
+#define WCNS_FLAG_SWEEP_WIDE 2
 
 typedef struct WcnsContext WcnsContext;
 
@@ -183,6 +189,10 @@ int wcns_launches_per_step(WcnsContext *ctx);
 int wcns_profile_step(WcnsContext *ctx, int cap, double *ms, const char **names, int *nphases);
 /* Number of points shared by more than two blocks (multi-point sets). */
 int wcns_n_multipoints(WcnsContext *ctx);
+/* How the context runs the LU-SGS sweeps: 0 clustered kernel (one thread-
+ * block cluster per block), 1 one launch per hyperplane, 2 wide cooperative
+ * sweeps (see WCNS_FLAG_SWEEP_BY_PLANE and WCNS_FLAG_SWEEP_WIDE). */
+int wcns_sweep_mode(WcnsContext *ctx);
 /* Failure-path self-test: runs the LU-SGS sweep's bounded wait (every wait
  * of the sweep kernels gives up after a clock-cycle limit instead of hanging)
  * on an mbarrier that nothing completes, with a limit of limit_cycles

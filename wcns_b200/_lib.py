@@ -49,6 +49,7 @@ SIGNATURES = {
     "wcns_stream": (C.c_void_p, [_VP]),
     "wcns_launches_per_step": (C.c_int, [_VP]),
     "wcns_n_multipoints": (C.c_int, [_VP]),
+    "wcns_sweep_mode": (C.c_int, [_VP]),
     "wcns_selftest_timeout": (C.c_int, [_VP, C.c_longlong]),
     "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
     "wcns_sa_setup": (C.c_int, [_VP, C.POINTER(C.c_void_p), C.c_double, C.c_double]),

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -100,6 +101,7 @@ struct WcnsContext {
     SaFields SA{};
     SaParams SAP{};
     int launches = 0;
+    std::unique_ptr<WideSweep> wide;
     ~WcnsContext() {
         if (graph) cudaGraphExecDestroy(graph);
         for (int q = 0; q < 2; q++) {
@@ -513,8 +515,33 @@ static int build_tables(WcnsContext *c) {
         int cl = 16, fine = 1;
         if (const char *e = getenv("WCNS_SWEEP_CLUSTER")) cl = atoi(e);
         if (const char *e = getenv("WCNS_SWEEP_FINE")) fine = atoi(e);
-        // blocks whose columns do not fit the clustered kernel sweep plane by plane
-        L.sweep_plane = (c->prm.flags & WCNS_FLAG_SWEEP_BY_PLANE) || setup_sweep(L, cl, fine) ? 1 : 0;
+        // blocks whose columns do not fit the clustered kernel run the wide
+        // cooperative sweeps, or, when those do not fit either, sweep plane by plane
+        const bool want_plane = c->prm.flags & WCNS_FLAG_SWEEP_BY_PLANE, want_wide = c->prm.flags & WCNS_FLAG_SWEEP_WIDE;
+        const bool clustered = !want_plane && !want_wide && setup_sweep(L, cl, fine) == 0;
+        if (!clustered && !want_plane) {
+            c->wide = std::make_unique<WideSweep>();
+            if (setup_sweep_wide(L, *c->wide) == 0) {
+                WideSweep &W = *c->wide;
+                WideArrays &A = W.A;
+                const size_t words = (size_t)(21 + 5 + 5 + 15 + 5) * A.n + 8;
+                CK(cudaMalloc(&A.stat, sizeof(double) * words));
+                c->owned.push_back(A.stat);
+                A.rhs = A.stat + (size_t)21 * A.n;
+                A.dql = A.rhs + (size_t)5 * A.n;
+                A.gs1 = A.dql + (size_t)5 * A.n;
+                A.gs2 = A.gs1 + (size_t)15 * A.n;
+                CK(cudaMalloc(&A.ring, sizeof(double) * (size_t)std::max(1, A.nbnd) * 8 * A.nkmax * 10));
+                c->owned.push_back(A.ring);
+                CK(cudaMalloc(&A.flags, sizeof(unsigned) * 2 * (size_t)std::max(1, A.nbnd)));
+                c->owned.push_back(A.flags);
+                W.chunks = c->up(W.hchunks);
+                L.wide = &W;
+            } else {
+                c->wide.reset();
+            }
+        }
+        L.sweep_plane = !clustered && !L.wide ? 1 : 0;
     }
     // residual partials, update bad lists
     L.res_ctas_per_block = 32;
@@ -672,7 +699,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
     }
     rc = build_tables(c);
     if (rc) { delete c; return rc; }
-    if (!L.sweep_plane) {
+    if (!L.sweep_plane && !L.wide) {
         // sweep arrays, plane-major: dq (5 planes of values), the static records
         // (SR_N per cell) and three dynamic records (DYN_N per cell); the memset
         // leaves zero the records that no kernel ever writes
@@ -1259,3 +1286,7 @@ extern "C" int wcns_launches_per_step(WcnsContext *c) {
     return c->launches;
 }
 extern "C" int wcns_n_multipoints(WcnsContext *c) { return c ? c->nmulti : 0; }
+extern "C" int wcns_sweep_mode(WcnsContext *c) {
+    if (!c) return -1;
+    return c->L.wide ? 2 : c->L.sweep_plane ? 1 : 0;
+}

@@ -691,6 +691,13 @@ int setup_sweep(LaunchCtx &c, int cluster, int fine) {
 
 int launch_lhs(const LaunchCtx &c) {
     const int zg = (int)((c.nzero + 255) / 256);
+    if (c.wide) {
+        if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
+        int n = launch_sweeps_wide(c);
+        if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);
+        prof_mark(c, "lhs_store");
+        return n + (c.nzero > 0 ? 2 : 0);
+    }
     if (c.sweep_plane) {
         // set_nonconnect_boundary_dq_0, the sweeps plane by plane, again the faces
         if (c.nzero > 0) k_zero_faces<<<zg, 256, 0, c.stream>>>(*c.F, c.zero_pts, c.nzero);

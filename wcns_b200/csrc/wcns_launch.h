@@ -1,6 +1,7 @@
 // wcns_launch.h -- host-side launch context shared by the kernel files.
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include "wcns_dev.cuh"
 
 namespace wcns {
@@ -74,6 +75,33 @@ struct ProfMarks {
     const char **name = nullptr;
 };
 
+// Wide sweeps (k_sweep_wide.cu): a chunk of whole j-rows of one block per
+// CTA, plane-major arrays, rings of planes between neighbouring chunks.
+constexpr int WIDE_MAX_THREADS = 576;
+struct WideChunk {
+    int blk, j0, w;         // block (0-based), first j-row (0-based) and width of the chunk
+    int bnd_lo, bnd_hi;     // ring between this chunk and the previous / next one (-1: none)
+    long long pmoff;        // the block's first slot in the plane-major arrays
+};
+struct WideArrays {
+    long long n = 0;        // slots per word array
+    double *stat = nullptr; // 21 words per slot: prim, metrics, sr, srv, coed
+    double *rhs = nullptr;  // 5
+    double *dql = nullptr;  // 5: lusgs_l's dq, the start of lusgs_u
+    double *gs1 = nullptr;  // 15: lusgs_u -> gs_pr_l, terms of the upper neighbours
+    double *gs2 = nullptr;  // 5: gs_pr_l -> gs_pr_u, summed terms of the lower neighbours
+    double *ring = nullptr; // [boundary][ring slot][nkmax][10]
+    unsigned *flags = nullptr;  // [boundary][produced, consumed] plane counts
+    int nbnd = 0, nkmax = 0;
+};
+struct WideSweep {
+    WideChunk *chunks = nullptr;  // device
+    std::vector<WideChunk> hchunks;
+    int nchunks = 0, threads = 0;
+    size_t smem_lu = 0, smem_gs = 0;
+    WideArrays A;
+};
+
 struct LaunchCtx {
     ProfMarks *prof = nullptr;
     cudaStream_t stream = 0;
@@ -128,6 +156,9 @@ struct LaunchCtx {
     // 1: the sweeps run as one launch per hyperplane on the field layout
     // (blocks too large for the clustered kernel, or asked for)
     int sweep_plane = 0;
+    // non-null: the sweeps run as wide cooperative sweeps (blocks too large
+    // for the clustered kernel)
+    WideSweep *wide = nullptr;
     const PmFields *PM = nullptr;  // plane-major sweep arrays
     // wall forces
     DevWall *walls = nullptr;
@@ -189,6 +220,8 @@ void launch_init_timestep(const LaunchCtx &c);
 void launch_communicate(const LaunchCtx &c, int which /*0 dq, 1 pv*/);
 int launch_lhs(const LaunchCtx &c);  // returns the number of launches
 int launch_sweeps_by_plane(const LaunchCtx &c);
+int setup_sweep_wide(LaunchCtx &c, WideSweep &W);  // -1: the blocks cannot be swept this way
+int launch_sweeps_wide(const LaunchCtx &c);
 int setup_sweep(LaunchCtx &c, int cluster, int fine);
 // the sweeps' bounded wait on an mbarrier nothing completes (self-test)
 void launch_wait_probe(const LaunchCtx &c, long long limit);

@@ -34,6 +34,7 @@ def _check(rc):
 
 
 FLAG_SWEEP_BY_PLANE = 1  # WCNS_FLAG_SWEEP_BY_PLANE
+FLAG_SWEEP_WIDE = 2  # WCNS_FLAG_SWEEP_WIDE
 
 
 def params_struct(p, flags=0) -> _lib.WcnsParams:
@@ -283,6 +284,10 @@ class Wcns:
         """The sweeps' bounded wait on an mbarrier nothing completes: raises
         WcnsError (WCNS_ERR_CUDA) as a step does after a sweep timeout."""
         _check(_lib.load().wcns_selftest_timeout(self.h, limit_cycles))
+
+    def sweep_mode(self) -> str:
+        """How the LU-SGS sweeps run: "clustered", "plane" or "wide"."""
+        return ("clustered", "plane", "wide")[int(_lib.load().wcns_sweep_mode(self.h))]
 
     def n_multipoints(self) -> int:
         return int(_lib.load().wcns_n_multipoints(self.h))
