@@ -207,14 +207,17 @@ def test_get_flow_is_the_interior():
 PLANE_CASES = ["vortex_roe_41", "plate_small", "plate_small_euler_wall", "supersonic_box_sw4"]
 
 
-@pytest.mark.parametrize("mode", ["plane", "wide"])
+@pytest.mark.parametrize("mode", ["plane", "wide", "wide_narrow"])
 @pytest.mark.parametrize("name", PLANE_CASES)
-def test_sweep_variants_match_oracle(name, mode):
+def test_sweep_variants_match_oracle(name, mode, monkeypatch):
     """The sweeps as one launch per hyperplane, and as wide cooperative
-    sweeps (on these small blocks every chunk is one j-row, so every j
-    contribution crosses a ring between CTAs)."""
+    sweeps: with the default chunking and with chunks of one j-row each
+    (WCNS_WIDE_MIN_COLS=1 on these small blocks), where every j contribution
+    crosses a ring between CTAs."""
     from oracle.pyoracle import Oracle
     from wcns_b200.solver import FLAG_SWEEP_BY_PLANE, FLAG_SWEEP_WIDE, Wcns
+    if mode == "wide_narrow":
+        monkeypatch.setenv("WCNS_WIDE_MIN_COLS", "1")
     case = CASES[name]()
     g, o = Wcns(case, flags=FLAG_SWEEP_BY_PLANE if mode == "plane" else FLAG_SWEEP_WIDE), Oracle(case)
     for gp, op in [("boundary_all", "boundary_all"), ("initial_q_dq_c_t", "initial_q_dq_c_t"),

@@ -405,3 +405,25 @@ def test_sa_rules_graph_steps(name):
     np.testing.assert_allclose(hg, ho, rtol=1e-12, atol=0)
     e = compare_fields(g, o, ["r", "u", "v", "w", "p", "qke", "vist"], region="all")
     assert max(e.values()) <= 1e-12, e
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("narrow", [False, True])
+def test_sa_wide_sweeps_graph_steps(narrow, monkeypatch):
+    """The reduced channel with the wide cooperative sweeps (the path of the
+    full channel), where the SA model's scalar LU-SGS runs on the same chunks:
+    whole steps against the oracle, qke and vist included; with narrow
+    chunks every j term crosses a ring between CTAs."""
+    from oracle.pyoracle import Oracle
+    from wcns_b200.solver import FLAG_SWEEP_WIDE, Wcns
+    if narrow:
+        monkeypatch.setenv("WCNS_WIDE_MIN_COLS", "1")
+    case = cases.small_channel_case()
+    g, o = Wcns(case, flags=FLAG_SWEEP_WIDE), Oracle(case)
+    assert g.sweep_mode() == "wide"
+    tt, km = case.sa["timedt_turb"], case.sa["kmaxlim"]
+    g.sa_setup(tt, km); o.sa_setup(tt, km)
+    hg, ho = g.step(5), o.step(5)
+    np.testing.assert_allclose(hg, ho, rtol=1e-12, atol=0)
+    e = compare_fields(g, o, ["r", "u", "v", "w", "p", "qke", "vist"], region="all")
+    assert max(e.values()) <= 1e-12, e

@@ -524,10 +524,10 @@ static int build_tables(WcnsContext *c) {
             if (setup_sweep_wide(L, *c->wide) == 0) {
                 WideSweep &W = *c->wide;
                 WideArrays &A = W.A;
-                const size_t words = (size_t)(21 + 5 + 5 + 15 + 5) * A.n + 8;
+                const size_t words = (size_t)(WIDE_COEF_WORDS + 5 + 5 + 15 + 5) * A.n + 8;
                 CK(cudaMalloc(&A.stat, sizeof(double) * words));
                 c->owned.push_back(A.stat);
-                A.rhs = A.stat + (size_t)21 * A.n;
+                A.rhs = A.stat + (size_t)WIDE_COEF_WORDS * A.n;
                 A.dql = A.rhs + (size_t)5 * A.n;
                 A.gs1 = A.dql + (size_t)5 * A.n;
                 A.gs2 = A.gs1 + (size_t)15 * A.n;
@@ -1028,6 +1028,12 @@ extern "C" int wcns_sa_setup(WcnsContext *c, const double *const *xyz, double ti
     S.kmaxlim = kmaxlim;
     c->L.SA = &c->SA;
     c->L.SAP = &c->SAP;
+    if (c->L.wide && !c->L.wide->A.sa) {
+        // the model's scalar sweeps run on the wide chunks too
+        WideArrays &A = c->L.wide->A;
+        CK(cudaMalloc(&A.sa, sizeof(double) * (6 * (size_t)A.n + 8)));
+        c->owned.push_back(A.sa);
+    }
     // the mean-flow kernels now read vist (spectvist, the viscous
     // coefficients); a step graph captured before holds the old arguments
     c->F.f[F_VIST] = c->SA.vist;
@@ -1153,7 +1159,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     launch_init_timestep(L); n += 1;
     prof_mark(L, "initial_q_dq_c_t+timestep");
     if (c->P.nvis == 1) {
-        if (c->sa_pool) { launch_turbulence(L); n += 4; }
+        if (c->sa_pool) n += launch_turbulence(L);
         launch_node_derivatives(L); n += 1;
         launch_rhs_dirs(L, true);
         for (int d = 0; d < 3; d++) n += L.vis[d].ngroups ? 1 : 0;

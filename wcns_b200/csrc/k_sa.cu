@@ -337,14 +337,17 @@ void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, 
         *c.SA, xyz, c.total, wall, nwall, c.blocks);
 }
 
-void launch_turbulence(const LaunchCtx &c) {
+int launch_turbulence(const LaunchCtx &c) {
     k_sa_point<SA_DMU><<<dim3(grid_for(max_points(c, 0)), c.nblocks), 256, 0, c.stream>>>(*c.F, *c.SA, *c.SAP, c.blocks);
     k_sa_point<SA_RHS><<<dim3(grid_for(max_points(c, 0)), c.nblocks), 256, 0, c.stream>>>(*c.F, *c.SA, *c.SAP, c.blocks);
     prof_mark(c, "sa_rhs");
-    k_sa_lusgs<<<c.nblocks, 1024, 0, c.stream>>>(*c.F, *c.SA, c.blocks);
+    // large blocks: the scalar sweeps on the wide chunks of the mean-flow sweeps
+    const int nl = (c.wide && c.wide->A.sa) ? launch_sa_lusgs_wide(c) : 1;
+    if (nl == 1) k_sa_lusgs<<<c.nblocks, 1024, 0, c.stream>>>(*c.F, *c.SA, c.blocks);
     prof_mark(c, "sa_lusgs");
     k_sa_point<SA_UPDATE><<<dim3(grid_for(max_points(c, 1)), c.nblocks), 256, 0, c.stream>>>(*c.F, *c.SA, *c.SAP, c.blocks);
     prof_mark(c, "sa_update");
+    return 3 + nl;
 }
 
 }  // namespace wcns

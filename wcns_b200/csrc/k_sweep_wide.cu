@@ -37,6 +37,7 @@
 // gs_pr_u ((del + dfl) + dgl, added first there).  gs_pr_u writes the result
 // to the field layout.
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "wcns_launch.h"
@@ -45,8 +46,26 @@ namespace wcns {
 
 namespace {
 
-enum : int { WS_R = 0, WS_M = 5, WS_SR = 14, WS_SRV = 17, WS_COED = 20, WS_N = 21 };
+// words per slot of the coefficient array: the direction-independent part of
+// the split Jacobian (um, vm, wm, hm, c2, af), per direction the normalised
+// metric and contravariant velocity (nx, ny, nz, ct), per direction and sign
+// (npn = +1 forward, -1 backward) l1, x1, x2, then coed and the three
+// viscous radii
+enum : int { WS_SH = 0, WS_D = 6, WS_P = 18, WS_MN = 27, WS_COED = 36, WS_SRV = 37, WS_N = 40 };
+static_assert(WS_N == WIDE_COEF_WORDS, "coefficient words per slot");
 constexpr int WIDE_RING = 8;
+constexpr int WIDE_PREFETCH = 3;  // planes prefetched into L2 ahead of the one being swept
+
+// The chunk's slots t = (k-1)*w + jj (j = j0+jj+1) that hold a cell of plane
+// p, i.e. 1 <= p-j-k <= ni: the first and last of them (the range between
+// may include slots outside the block).  False when there is none.
+__host__ __device__ __forceinline__ bool active_slots(int p, int j0, int w, int ni, int nk, int &lo, int &hi) {
+    const int klo = max(1, p - ni - j0 - w), khi = min(nk, p - 2 - j0);
+    if (klo > khi) return false;
+    lo = (klo - 1) * w + max(0, p - ni - klo - j0 - 1);
+    hi = (khi - 1) * w + min(w - 1, p - khi - j0 - 2);
+    return lo <= hi;
+}
 
 struct Jsc {  // split-Jacobian coefficients of a cell along one direction (one sign)
     double nx, ny, nz, ct, l1, x1, x2;
@@ -55,9 +74,10 @@ struct Jsh {  // direction-independent part
     double um, vm, wm, hm, c2, af;
 };
 
-// the dq-independent part of mxdq_std (gettmhmgm_ns GasModel.f90:411-426, nt = 0)
+// the dq-independent part of mxdq_std (gettmhmgm_ns GasModel.f90:411-426,
+// nt = 0) from s = prim (5), the nine metrics, the three inviscid radii
 __device__ __forceinline__ void jac_coeffs(double gama, const double *s, int d, double npn, Jsh &H, Jsc &J) {
-    const double rm = s[WS_R], um = s[WS_R + 1], vm = s[WS_R + 2], wm = s[WS_R + 3], pm = s[WS_R + 4];
+    const double rm = s[0], um = s[1], vm = s[2], wm = s[3], pm = s[4];
     const double nt = 0.0;
     const double hint = gama / (gama - 1.0) * pm / rm;
     const double c2 = gama * pm / rm;
@@ -70,8 +90,8 @@ __device__ __forceinline__ void jac_coeffs(double gama, const double *s, int d, 
     H.c2 = c2;
     const double ae = gama - 1.0;
     H.af = 0.5 * ae * v2;
-    double nx = s[WS_M + 3 * d], ny = s[WS_M + 3 * d + 1], nz = s[WS_M + 3 * d + 2];
-    const double rad = s[WS_SR + d];
+    double nx = s[5 + 3 * d], ny = s[5 + 3 * d + 1], nz = s[5 + 3 * d + 2];
+    const double rad = s[14 + d];
     double ct = nx * um + ny * vm + nz * wm + nt;
     double cgm = sqrt(nx * nx + ny * ny + nz * nz);
     if (!(cgm >= SML_SSS)) cgm = SML_SSS;
@@ -128,50 +148,78 @@ __device__ __forceinline__ void prefetch_l2(const double *ptr, int n) {
 
 }  // namespace
 
-// plane-major copy of everything the sweeps read that does not depend on dq
-// (set_nonconnect_boundary_dq_0 has run, so rhs already holds the zeros of
-// the physical faces); one thread per slot
+// plane-major coefficients of every cell, evaluated once per step for all
+// four sweeps: the dq-independent part of mxdq_std for the cell acting as a
+// neighbour (getrkec_mml and getrarbrc return the cell's own metrics and
+// spectral radius for interior cells) for both signs, coed (getcoed,
+// 602-645), the viscous radii, and rhs = dq (set_nonconnect_boundary_dq_0
+// has run, so rhs holds the zeros of the physical faces); one thread per slot
 __global__ void __launch_bounds__(256) k_wide_prep(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                   const WideChunk *__restrict__ chunks, WideArrays A) {
     const WideChunk C = chunks[blockIdx.y];
     const DevBlock B = blocks[C.blk];
     const int ncolc = C.w * B.nk, np = B.ni + B.nj + B.nk - 2;
     const long long n = (long long)np * ncolc;
+    const double gama = P.gama;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const int s = (int)(e / ncolc), t = (int)(e - (long long)s * ncolc);
         const int p = s + 3, j = C.j0 + t % C.w + 1, k = t / C.w + 1, i = p - j - k;
         if (i < 1 || i > B.ni) continue;
         const long long id = gidx(B, i, j, k);
         const long long pm = C.pmoff + (long long)s * (B.nj * B.nk) + (long long)C.j0 * B.nk + t;
+        double *o = A.stat + pm;
+        const size_t N = (size_t)A.n;
+        double st[21];  // prim, metrics, inviscid radii
 #pragma unroll
-        for (int m = 0; m < 5; m++) A.stat[(size_t)(WS_R + m) * A.n + pm] = F.f[F_R + m][id];
+        for (int m = 0; m < 5; m++) st[m] = F.f[F_R + m][id];
 #pragma unroll
-        for (int m = 0; m < 9; m++) A.stat[(size_t)(WS_M + m) * A.n + pm] = F.f[F_KCX + m][id];
+        for (int m = 0; m < 9; m++) st[5 + m] = F.f[F_KCX + m][id];
 #pragma unroll
-        for (int m = 0; m < 3; m++) {
-            A.stat[(size_t)(WS_SR + m) * A.n + pm] = F.f[F_SRA + m][id];
-            A.stat[(size_t)(WS_SRV + m) * A.n + pm] = F.f[F_SRVA + m][id];
+        for (int m = 0; m < 3; m++) st[14 + m] = F.f[F_SRA + m][id];
+        Jsh H;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            Jsc Jp, Jm;
+            jac_coeffs(gama, st, d, 1.0, H, Jp);
+            jac_coeffs(gama, st, d, -1.0, H, Jm);
+            o[(WS_D + 4 * d + 0) * N] = Jp.nx;
+            o[(WS_D + 4 * d + 1) * N] = Jp.ny;
+            o[(WS_D + 4 * d + 2) * N] = Jp.nz;
+            o[(WS_D + 4 * d + 3) * N] = Jp.ct;
+            o[(WS_P + 3 * d + 0) * N] = Jp.l1;
+            o[(WS_P + 3 * d + 1) * N] = Jp.x1;
+            o[(WS_P + 3 * d + 2) * N] = Jp.x2;
+            o[(WS_MN + 3 * d + 0) * N] = Jm.l1;
+            o[(WS_MN + 3 * d + 1) * N] = Jm.x1;
+            o[(WS_MN + 3 * d + 2) * N] = Jm.x2;
         }
+        o[(WS_SH + 0) * N] = H.um;
+        o[(WS_SH + 1) * N] = H.vm;
+        o[(WS_SH + 2) * N] = H.wm;
+        o[(WS_SH + 3) * N] = H.hm;
+        o[(WS_SH + 4) * N] = H.c2;
+        o[(WS_SH + 5) * N] = H.af;
         // getcoed (LHS.f90:602-645), wmig = beta = 1, no dual time stepping
         double rad_ns = F.f[F_SRA][id] + F.f[F_SRB][id] + F.f[F_SRC][id];
         if (P.nvis >= 1) rad_ns = rad_ns + F.f[F_SRVA][id] + F.f[F_SRVB][id] + F.f[F_SRVC][id];
         const double ct = 1.0 / F.f[F_DTDT][id];
-        A.stat[(size_t)WS_COED * A.n + pm] = 1.0 / (ct + 1.0 * 1.0 * rad_ns);
+        o[WS_COED * N] = 1.0 / (ct + 1.0 * 1.0 * rad_ns);
 #pragma unroll
-        for (int m = 0; m < 5; m++) A.rhs[(size_t)m * A.n + pm] = F.f[F_DQ1 + m][id];
+        for (int m = 0; m < 3; m++) o[(WS_SRV + m) * N] = F.f[F_SRVA + m][id];
+#pragma unroll
+        for (int m = 0; m < 5; m++) A.rhs[(size_t)m * N + pm] = F.f[F_DQ1 + m][id];
     }
 }
 
 // MODE 0 lusgs_l, 1 lusgs_u, 2 gs_pr_l, 3 gs_pr_u
 template <int MODE>
-__global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sweep_wide(DevParams P, DevFields F,
+__global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F,
                                                                     const DevBlock *__restrict__ blocks,
                                                                     const WideChunk *__restrict__ chunks, WideArrays A,
                                                                     int *err) {
     constexpr bool FWD = MODE == 0 || MODE == 2;
     constexpr bool LU = MODE <= 1;
     constexpr int NC = LU ? 10 : 5;  // pushed values: A*dq (5) and, in lusgs, srv*dq (5)
-    const double npn = FWD ? 1.0 : -1.0;
     const WideChunk C = chunks[blockIdx.x];
     const DevBlock B = blocks[C.blk];
     const int t = threadIdx.x, ncolc = C.w * B.nk, ncol = B.nj * B.nk;
@@ -203,19 +251,24 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sweep_wide(DevParams P,
     for (int m = 0; m < NC; m++) ibuf[m] = 0.0;
     const int pfirst = FWD ? 3 : B.ni + B.nj + B.nk;
     const int pstep = FWD ? 1 : -1;
-    const double *warr[4] = {A.stat, A.rhs, MODE == 1 ? A.dql : nullptr, MODE == 2 ? A.gs1 : MODE == 3 ? A.gs2 : nullptr};
-    const int wcnt[4] = {WS_N, 5, MODE == 1 ? 5 : 0, MODE == 2 ? 15 : MODE == 3 ? 5 : 0};
+    // the words this sweep reads: [first word, count] runs of the coefficient
+    // array, then the start values and the stored Gauss-Seidel terms
+    const int sg = FWD ? WS_P : WS_MN;
+    const double *warr[6] = {A.stat + (size_t)WS_SH * A.n, A.stat + (size_t)sg * A.n,
+                             A.stat + (size_t)WS_COED * A.n, MODE == 1 ? A.dql : A.rhs,
+                             MODE == 2 ? A.gs1 : MODE == 3 ? A.gs2 : nullptr, nullptr};
+    const int wcnt[6] = {WS_D + 12 - WS_SH, 9, LU ? 4 : 1, 5, MODE == 2 ? 15 : MODE == 3 ? 5 : 0, 0};
     auto prefetch_plane = [&](int s) {
         if (s >= np) return;
         const int p = pfirst + s * pstep;
-        const long long pm0 = C.pmoff + (long long)(p - 3) * ncol + (long long)C.j0 * B.nk;
-        for (int a = 0; a < 4; a++)
-            for (int w = 0; w < wcnt[a]; w++) prefetch_l2(warr[a] + (size_t)w * A.n + pm0, ncolc);
+        int lo, hi;
+        if (!active_slots(p, C.j0, C.w, B.ni, B.nk, lo, hi)) return;
+        const long long pm0 = C.pmoff + (long long)(p - 3) * ncol + (long long)C.j0 * B.nk + lo;
+        for (int a = 0; a < 5; a++)
+            for (int w = 0; w < wcnt[a]; w++) prefetch_l2(warr[a] + (size_t)w * A.n + pm0, hi - lo + 1);
     };
-    if (t == 0) {
-        prefetch_plane(0);
-        prefetch_plane(1);
-    }
+    if (t == 0)
+        for (int a = 0; a < WIDE_PREFETCH; a++) prefetch_plane(a);
     for (int s = 0; s < np; s++) {
         const int p = pfirst + s * pstep;
         const int i = p - j - k;
@@ -227,25 +280,41 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sweep_wide(DevParams P,
         Jsc J[3];
         double base[5], coed = 0.0, rv[3] = {0.0, 0.0, 0.0};
         if (act) {
-            double st[WS_N];
+            const double *cf = A.stat + pm;
+            const size_t N = (size_t)A.n;
+            const int sg = FWD ? WS_P : WS_MN;
+            H.um = cf[(WS_SH + 0) * N];
+            H.vm = cf[(WS_SH + 1) * N];
+            H.wm = cf[(WS_SH + 2) * N];
+            H.hm = cf[(WS_SH + 3) * N];
+            H.c2 = cf[(WS_SH + 4) * N];
+            H.af = cf[(WS_SH + 5) * N];
 #pragma unroll
-            for (int w = 0; w < WS_N; w++) st[w] = A.stat[(size_t)w * A.n + pm];
+            for (int d = 0; d < 3; d++) {
+                J[d].nx = cf[(WS_D + 4 * d + 0) * N];
+                J[d].ny = cf[(WS_D + 4 * d + 1) * N];
+                J[d].nz = cf[(WS_D + 4 * d + 2) * N];
+                J[d].ct = cf[(WS_D + 4 * d + 3) * N];
+                J[d].l1 = cf[(sg + 3 * d + 0) * N];
+                J[d].x1 = cf[(sg + 3 * d + 1) * N];
+                J[d].x2 = cf[(sg + 3 * d + 2) * N];
+            }
+            coed = cf[WS_COED * N];
+            if (LU) {
 #pragma unroll
-            for (int d = 0; d < 3; d++) jac_coeffs(gama, st, d, npn, H, J[d]);
-            coed = st[WS_COED];
-#pragma unroll
-            for (int d = 0; d < 3; d++) rv[d] = st[WS_SRV + d];
+                for (int d = 0; d < 3; d++) rv[d] = cf[(WS_SRV + d) * N];
+            }
             const double *bsrc = MODE == 1 ? A.dql : A.rhs;
 #pragma unroll
             for (int m = 0; m < 5; m++) base[m] = bsrc[(size_t)m * A.n + pm];
         }
         if (t == 0) {
-            prefetch_plane(s + 2);
+            prefetch_plane(s + WIDE_PREFETCH);
             if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit())) timed_out = true;
             if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit())) timed_out = true;
         }
         __syncthreads();  // the previous plane's inbox and ring entries are complete
-        if (t == 0) {
+        if (t == 0 && (ring_out || ring_in)) {
             __threadfence();
             if (ring_out && s > 0) st_release(prod_out, (unsigned)s);      // planes 0..s-1 published
             if (ring_in && s > 1) st_release(cons_in, (unsigned)(s - 1));  // planes 0..s-2 read
@@ -377,6 +446,8 @@ int setup_sweep_wide(LaunchCtx &c, WideSweep &W) {
         nkmax = std::max(nkmax, c.hblocks[b].nk);
     }
     if (nkmax > WIDE_MAX_THREADS) return -1;
+    int min_cols = 128;
+    if (const char *e = getenv("WCNS_WIDE_MIN_COLS")) min_cols = std::max(1, atoi(e));  // tests: narrow chunks
     // columns per chunk: start from an even share of the SMs and widen the
     // chunks until every CTA of the launch fits on the device at once
     for (long long target = std::max<long long>(1, (cols + nsm - 1) / nsm);; target = target + target / 25 + 1) {
@@ -387,7 +458,9 @@ int setup_sweep_wide(LaunchCtx &c, WideSweep &W) {
         for (int b = 0; b < c.nblocks; b++) {
             const DevBlock &B = c.hblocks[b];
             int w = (int)std::max<long long>(1, std::min<long long>(target / B.nk, WIDE_MAX_THREADS / B.nk));
-            w = std::min(w, B.nj);
+            // at least min_cols columns per chunk: every chunk edge adds a hop between SMs per plane
+            w = std::max(w, std::min((min_cols + B.nk - 1) / B.nk, WIDE_MAX_THREADS / B.nk));
+            w = std::max(1, std::min(w, B.nj));
             const int G = (B.nj + w - 1) / w;
             pmoff[b] = n;
             n += (long long)(B.ni + B.nj + B.nk - 2) * B.nj * B.nk;
@@ -476,6 +549,167 @@ int launch_sweeps_wide(const LaunchCtx &c) {
     launch_wide_t<3>(c);
     prof_mark(c, "sweep_gs_pr_u");
     return n + 4;
+}
+
+
+// ---------------------------------------------------------------------------
+// lusgs_turbulence (turblence.f90:477-558) on the same chunks: the SA model's
+// scalar forward and backward sweeps over the points 2..n-1 of every
+// direction.  A point's term for a successor is mxdq_std_turbulence
+// (560-583) of the point itself: 0.5*(l + npn*|l|)*dqke with l the
+// contravariant velocity along the direction, so the prep keeps l for the
+// three directions, spec and the right-hand side per slot.
+
+// sa words per slot: l along i, j, k; spec; dqke (right-hand side); the forward result
+enum : int { WSA_L = 0, WSA_SPEC = 3, WSA_RHS = 4, WSA_FWD = 5, WSA_N = 6 };
+
+__global__ void __launch_bounds__(256) k_sa_wide_prep(DevFields F, SaFields S, const DevBlock *__restrict__ blocks,
+                                                     const WideChunk *__restrict__ chunks, WideArrays A) {
+    const WideChunk C = chunks[blockIdx.y];
+    const DevBlock B = blocks[C.blk];
+    const int ncolc = C.w * B.nk, np = B.ni + B.nj + B.nk - 2;
+    const long long n = (long long)np * ncolc;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(e / ncolc), t = (int)(e - (long long)s * ncolc);
+        const int p = s + 3, j = C.j0 + t % C.w + 1, k = t / C.w + 1, i = p - j - k;
+        if (i < 2 || i > B.ni - 1 || j < 2 || j > B.nj - 1 || k < 2 || k > B.nk - 1) continue;
+        const long long id = gidx(B, i, j, k);
+        const long long pm = C.pmoff + (long long)s * (B.nj * B.nk) + (long long)C.j0 * B.nk + t;
+        const double u = F.f[F_U][id], v = F.f[F_V][id], w = F.f[F_W][id];
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            A.sa[(size_t)(WSA_L + d) * A.n + pm] =
+                F.f[F_KCX + 3 * d][id] * u + F.f[F_KCX + 3 * d + 1][id] * v + F.f[F_KCX + 3 * d + 2][id] * w;
+        A.sa[(size_t)WSA_SPEC * A.n + pm] = S.spec[id];
+        A.sa[(size_t)WSA_RHS * A.n + pm] = S.dqke[id];
+    }
+}
+
+template <bool FWD>
+__global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields S, const DevBlock *__restrict__ blocks,
+                                                                       const WideChunk *__restrict__ chunks,
+                                                                       WideArrays A, int *err) {
+    const double npn = FWD ? 1.0 : -1.0;
+    const WideChunk C = chunks[blockIdx.x];
+    const DevBlock B = blocks[C.blk];
+    const int t = threadIdx.x, ncolc = C.w * B.nk, ncol = B.nj * B.nk;
+    const bool own = t < ncolc;
+    const int jj = own ? t % C.w : 0;
+    const int j = C.j0 + jj + 1, k = own ? t / C.w + 1 : 1;
+    const bool colin = own && j >= 2 && j <= B.nj - 1 && k >= 2 && k <= B.nk - 1;
+    const int np = B.ni + B.nj + B.nk - 2;
+    const int rin = FWD ? C.bnd_lo : C.bnd_hi, rout = FWD ? C.bnd_hi : C.bnd_lo;
+    const bool jedge_in = FWD ? jj == 0 : jj == C.w - 1;
+    const bool jedge_out = FWD ? jj == C.w - 1 : jj == 0;
+    // a predecessor outside 2..n-1 contributes zero (its dqke is zero)
+    const bool hasj = FWD ? j > 2 : j < B.nj - 1;
+    const bool hask = FWD ? k > 2 : k < B.nk - 1;
+    __shared__ double inbox[2][2][WIDE_MAX_THREADS];
+    double *const ring_in = rin >= 0 ? A.ring + (size_t)rin * WIDE_RING * A.nkmax * 10 : nullptr;
+    double *const ring_out = rout >= 0 ? A.ring + (size_t)rout * WIDE_RING * A.nkmax * 10 : nullptr;
+    unsigned *const prod_in = rin >= 0 ? A.flags + 2 * rin : nullptr, *const cons_in = prod_in ? prod_in + 1 : nullptr;
+    unsigned *const prod_out = rout >= 0 ? A.flags + 2 * rout : nullptr, *const cons_out = prod_out ? prod_out + 1 : nullptr;
+    bool timed_out = false;
+    auto limit = [&]() { return timed_out ? (1LL << 21) : (1LL << 31); };
+    double ibuf = 0.0;
+    const int pfirst = FWD ? 3 : B.ni + B.nj + B.nk, pstep = FWD ? 1 : -1;
+    auto prefetch_plane = [&](int s) {
+        if (s >= np) return;
+        const int p = pfirst + s * pstep;
+        int lo, hi;
+        if (!active_slots(p, C.j0, C.w, B.ni, B.nk, lo, hi)) return;
+        const long long pm0 = C.pmoff + (long long)(p - 3) * ncol + (long long)C.j0 * B.nk + lo;
+        for (int w = 0; w < WSA_N; w++) prefetch_l2(A.sa + (size_t)w * A.n + pm0, hi - lo + 1);
+    };
+    if (t == 0)
+        for (int a = 0; a < WIDE_PREFETCH; a++) prefetch_plane(a);
+    for (int s = 0; s < np; s++) {
+        const int p = pfirst + s * pstep;
+        const int i = p - j - k;
+        const bool act = colin && i >= 2 && i <= B.ni - 1;
+        const bool hasi = FWD ? i > 2 : i < B.ni - 1;
+        const long long pm = C.pmoff + (long long)(p - 3) * ncol + (long long)C.j0 * B.nk + t;
+        double l[3] = {0.0, 0.0, 0.0}, spec = 1.0, base = 0.0;
+        if (act) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double ct = A.sa[(size_t)(WSA_L + d) * A.n + pm];
+                l[d] = 0.5 * (ct + npn * fabs(ct));
+            }
+            spec = A.sa[(size_t)WSA_SPEC * A.n + pm];
+            base = A.sa[(size_t)(FWD ? WSA_RHS : WSA_FWD) * A.n + pm];
+        }
+        if (t == 0) {
+            prefetch_plane(s + WIDE_PREFETCH);
+            if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit())) timed_out = true;
+            if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit())) timed_out = true;
+        }
+        __syncthreads();
+        if (t == 0 && (ring_out || ring_in)) {
+            __threadfence();
+            if (ring_out && s > 0) st_release(prod_out, (unsigned)s);
+            if (ring_in && s > 1) st_release(cons_in, (unsigned)(s - 1));
+        }
+        if (!act) continue;
+        const int rp = (s + 1) & 1, wp = s & 1;
+        const double ti = hasi ? ibuf : 0.0;
+        double tj = 0.0, tk = 0.0;
+        if (hasj) {
+            if (jedge_in) tj = __ldcg(ring_in + ((size_t)((s - 1) % WIDE_RING) * A.nkmax + (k - 1)) * 10);
+            else tj = inbox[rp][0][FWD ? t - 1 : t + 1];
+        }
+        if (hask) tk = inbox[rp][1][FWD ? t - C.w : t + C.w];
+        const double rhs0 = ti + tj + tk;
+        const double nw = FWD ? (rhs0 - base) / spec : base - rhs0 / spec;
+        if (FWD) A.sa[(size_t)WSA_FWD * A.n + pm] = nw;
+        else S.dqke[gidx(B, i, j, k)] = nw;
+        ibuf = l[0] * nw;
+        inbox[wp][0][t] = l[1] * nw;
+        inbox[wp][1][t] = l[2] * nw;
+        if (jedge_out && ring_out) __stcg(ring_out + ((size_t)(s % WIDE_RING) * A.nkmax + (k - 1)) * 10, l[1] * nw);
+    }
+    __syncthreads();
+    if (t == 0) {
+        __threadfence();
+        if (ring_out) st_release(prod_out, (unsigned)np);
+        if (ring_in) st_release(cons_in, (unsigned)np);
+        if (timed_out) atomicAdd(&err[ERR_TIMEOUT], 1);
+    }
+}
+
+template <bool FWD>
+static void launch_sa_wide_t(const LaunchCtx &c) {
+    const WideSweep &W = *c.wide;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(W.nchunks, 1, 1);
+    cfg.blockDim = dim3(W.threads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.stream;
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_sa_sweep_wide<FWD>, *c.SA, (const DevBlock *)c.blocks, (const WideChunk *)W.chunks, W.A,
+                       c.err);
+}
+
+// the SA model's scalar LU-SGS on the wide chunks; returns the number of launches
+int launch_sa_lusgs_wide(const LaunchCtx &c) {
+    const WideSweep &W = *c.wide;
+    int maxslots = 0;
+    for (const WideChunk &C : W.hchunks) {
+        const DevBlock &B = c.hblocks[C.blk];
+        maxslots = std::max(maxslots, (B.ni + B.nj + B.nk - 2) * C.w * B.nk);
+    }
+    k_sa_wide_prep<<<dim3((unsigned)std::min(4096, (maxslots + 255) / 256), W.nchunks), 256, 0, c.stream>>>(
+        *c.F, *c.SA, c.blocks, W.chunks, W.A);
+    const size_t fbytes = sizeof(unsigned) * 2 * (size_t)std::max(1, W.A.nbnd);
+    cudaMemsetAsync(W.A.flags, 0, fbytes, c.stream);
+    launch_sa_wide_t<true>(c);
+    cudaMemsetAsync(W.A.flags, 0, fbytes, c.stream);
+    launch_sa_wide_t<false>(c);
+    return 3;
 }
 
 }  // namespace wcns

@@ -78,6 +78,8 @@ struct ProfMarks {
 // Wide sweeps (k_sweep_wide.cu): a chunk of whole j-rows of one block per
 // CTA, plane-major arrays, rings of planes between neighbouring chunks.
 constexpr int WIDE_MAX_THREADS = 576;
+constexpr int WIDE_MAX_REGS = 112;  // 18 warps x 32 x 112 registers fit one SM's register file
+constexpr int WIDE_COEF_WORDS = 40;  // coefficient words per slot (k_sweep_wide.cu)
 struct WideChunk {
     int blk, j0, w;         // block (0-based), first j-row (0-based) and width of the chunk
     int bnd_lo, bnd_hi;     // ring between this chunk and the previous / next one (-1: none)
@@ -85,11 +87,12 @@ struct WideChunk {
 };
 struct WideArrays {
     long long n = 0;        // slots per word array
-    double *stat = nullptr; // 21 words per slot: prim, metrics, sr, srv, coed
+    double *stat = nullptr; // WIDE_COEF_WORDS per slot: split-Jacobian coefficients, coed, srv
     double *rhs = nullptr;  // 5
     double *dql = nullptr;  // 5: lusgs_l's dq, the start of lusgs_u
     double *gs1 = nullptr;  // 15: lusgs_u -> gs_pr_l, terms of the upper neighbours
     double *gs2 = nullptr;  // 5: gs_pr_l -> gs_pr_u, summed terms of the lower neighbours
+    double *sa = nullptr;   // 6: the SA model's scalar sweeps (after wcns_sa_setup)
     double *ring = nullptr; // [boundary][ring slot][nkmax][10]
     unsigned *flags = nullptr;  // [boundary][produced, consumed] plane counts
     int nbnd = 0, nkmax = 0;
@@ -222,6 +225,7 @@ int launch_lhs(const LaunchCtx &c);  // returns the number of launches
 int launch_sweeps_by_plane(const LaunchCtx &c);
 int setup_sweep_wide(LaunchCtx &c, WideSweep &W);  // -1: the blocks cannot be swept this way
 int launch_sweeps_wide(const LaunchCtx &c);
+int launch_sa_lusgs_wide(const LaunchCtx &c);  // needs wide->A.sa
 int setup_sweep(LaunchCtx &c, int cluster, int fine);
 // the sweeps' bounded wait on an mbarrier nothing completes (self-test)
 void launch_wait_probe(const LaunchCtx &c, long long limit);
@@ -233,6 +237,6 @@ void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
 // SA model: set-up (init_SA and the wall distance; xyz: 3 fields of the
 // pool's layout, wall: 3 doubles per wall point) and one model step
 void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, int nwall, double vt);
-void launch_turbulence(const LaunchCtx &c);
+int launch_turbulence(const LaunchCtx &c);  // returns the number of launches
 
 }  // namespace wcns
