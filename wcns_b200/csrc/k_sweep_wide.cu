@@ -37,6 +37,7 @@
 // gs_pr_u ((del + dfl) + dgl, added first there).  gs_pr_u writes the result
 // to the field layout.
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <vector>
 
@@ -480,16 +481,25 @@ int setup_sweep_wide(LaunchCtx &c, WideSweep &W) {
         }
         const int threads = (maxcols + 31) / 32 * 32;
         const size_t smem = wide_smem_bytes(maxcols, 10);
-        if (threads > WIDE_MAX_THREADS || smem > 227 * 1024) return -1;
+        const bool verbose = getenv("WCNS_VERBOSE") != nullptr;
+        if (threads > WIDE_MAX_THREADS || smem > 227 * 1024) {
+            if (verbose) fprintf(stderr, "wide sweeps: %d threads, %zu bytes of shared memory per CTA do not fit\n", threads, smem);
+            return -1;
+        }
         int per_sm = 0;
         cudaFuncSetAttribute(k_sweep_wide<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_sweep_wide<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_sweep_wide<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_sweep_wide<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_wide<0>, threads, smem) != cudaSuccess) {
+        const cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_wide<0>, threads, smem);
+        if (oe != cudaSuccess) {
+            if (verbose) fprintf(stderr, "wide sweeps: occupancy query failed: %s\n", cudaGetErrorString(oe));
             cudaGetLastError();
             return -1;
         }
+        if (verbose)
+            fprintf(stderr, "wide sweeps: %zu chunks, %d threads, %zu bytes of shared memory, %d CTAs per SM on %d SMs\n",
+                    ch.size(), threads, smem, per_sm, nsm);
         if ((long long)per_sm * nsm < (long long)ch.size()) {
             if (threads >= WIDE_MAX_THREADS) return -1;
             continue;
