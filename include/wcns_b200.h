@@ -161,6 +161,21 @@ int wcns_turbulence(WcnsContext *ctx);
  * ref = {sref, lfref, xref, yref, zref, nwholefield} (param.dat $force);
  * out = {cfx, cfy, cfz, cmx, cmy, cmz, cl, cd, xcp}. */
 int wcns_forces(WcnsContext *ctx, const double *ref, double *out);
+/* The same over the wall regions of blocks nb0..nb1 only: the forces of one
+ * case when independent cases share a context. */
+int wcns_forces_blocks(WcnsContext *ctx, int nb0, int nb1, const double *ref, double *out);
+
+/* Several independent cases in one context: their blocks and BC records are
+ * concatenated for wcns_create (block numbers renumbered, no interface
+ * between cases), the parameters of wcns_create are common to all of them,
+ * and a case at another Mach number sets it on each of its blocks here: the
+ * free-stream pressure, speed of sound and the Mach-dependent constants of
+ * init_inflow (PreProcess.f90:968-1113) used by the BCs, T, the heat-flux
+ * coefficients and the wall forces.  The SA model's wall distance is measured
+ * within each set of blocks joined through interfaces, i.e. within a case.
+ * A batch of small cases then runs as one launch per kernel.  No counterpart
+ * in the reference, which runs one case per job. */
+int wcns_set_block_freestream(WcnsContext *ctx, int nb, double moo);
 
 /* The whole step of Main.f90:85-109 repeated nsteps times, replayed from a
  * CUDA graph.  rms_history (may be NULL) receives the residual RMS of every

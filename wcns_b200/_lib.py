@@ -52,6 +52,8 @@ SIGNATURES = {
     "wcns_sweep_mode": (C.c_int, [_VP]),
     "wcns_selftest_timeout": (C.c_int, [_VP, C.c_longlong]),
     "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
+    "wcns_forces_blocks": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
+    "wcns_set_block_freestream": (C.c_int, [_VP, C.c_int, C.c_double]),
     "wcns_sa_setup": (C.c_int, [_VP, C.POINTER(C.c_void_p), C.c_double, C.c_double]),
     "wcns_turbulence": (C.c_int, [_VP]),
     "wcns_residual_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p), _VP, _VP, _VP, _VP]),

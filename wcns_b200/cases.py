@@ -64,6 +64,10 @@ class Case:
     # Spalart-Allmaras settings ($step timedt_turb, $turbulence kmaxlim) for
     # nlamtur=1, nameturb='SA' runs; None for laminar/Euler cases
     sa: dict | None = None
+    # a batch of independent cases in one context: each block's Mach number
+    # (None: params.moo everywhere) and each case's block range (nb0, nb1)
+    block_moo: list | None = None
+    groups: list | None = None
 
     @property
     def npoints(self) -> int:
@@ -463,5 +467,52 @@ def small_channel_case(**kw) -> Case:
     return channel_case(**args)
 
 
+def batch_case(ncases=64, seed=0, nsteps=50) -> Case:
+    """Independent small channel cases with a wall bump, one block each, for
+    one batched context: block sizes drawn from 17^3 .. 49x33x17, Mach from
+    U[0.3, 0.8], bump height (fraction of the channel height) from
+    U[0.02, 0.08], by seed.  The common parameters are those of the SA
+    channel (Re_H 5e6, adiabatic walls, far-field inlet and outlet, spanwise
+    symmetry); every case keeps its own Mach number through block_moo and its
+    blocks (here one) through groups."""
+    rng = np.random.default_rng(seed)
+    dims, xyz, prim, regs, moo, groups = [], [], [], [], [], []
+    first = None
+    for c in range(ncases):
+        ni, nj, nk = int(rng.integers(17, 50)), int(rng.integers(17, 34)), 17
+        m, h = float(rng.uniform(0.3, 0.8)), float(rng.uniform(0.02, 0.08))
+        one = channel_case(ni=ni, nj=nj, nk=nk, bx=1, by=1, bz=1, bump=h, first=1.0e-3, seed=seed + c)
+        one.params.moo = m
+        if first is None:
+            first = one
+        nb = len(dims) + 1
+        dims += one.dims
+        xyz += one.xyz
+        prim.append(tuple(freestream_prim(one.params, one.dims[0])))
+        r = one.regions.copy()
+        r[:, 0] += nb - 1
+        r[:, 14] = np.where(r[:, 7] < 0, r[:, 14] + nb - 1, r[:, 14])
+        regs.append(r)
+        moo.append(m)
+        groups.append((nb, nb + len(one.dims) - 1))
+    npts = sum(a * b * c for a, b, c in dims)
+    return Case("batch", first.params, dims, xyz, np.concatenate(regs), prim, nsteps,
+                f"{ncases} independent SA bump cases, one block each, {npts} points",
+                sa=first.sa, block_moo=moo, groups=groups)
+
+
+def batch_member(case: Case, q: int) -> Case:
+    """Case q of a batch as a case of its own (its blocks, BC records and Mach)."""
+    nb0, nb1 = case.groups[q]
+    sel = (case.regions[:, 0] >= nb0) & (case.regions[:, 0] <= nb1)
+    r = case.regions[sel].copy()
+    r[:, 0] -= nb0 - 1
+    r[:, 14] = np.where(r[:, 7] < 0, r[:, 14] - (nb0 - 1), r[:, 14])
+    prm = Params(**{k: getattr(case.params, k) for k in Params.__dataclass_fields__})
+    prm.moo = case.block_moo[nb0 - 1]
+    return Case(f"{case.name}_{q}", prm, case.dims[nb0 - 1:nb1], case.xyz[nb0 - 1:nb1], r,
+                [tuple(a.copy() for a in p) for p in case.prim[nb0 - 1:nb1]], case.nsteps, "", sa=case.sa)
+
+
 CASES = {"vortex": vortex_case, "plate": plate_case, "small_plate": small_plate_case,
-         "channel": channel_case, "small_channel": small_channel_case}
+         "channel": channel_case, "small_channel": small_channel_case, "batch": batch_case}

@@ -102,6 +102,7 @@ struct WcnsContext {
     SaParams SAP{};
     int launches = 0;
     std::unique_ptr<WideSweep> wide;
+    std::vector<DevWall> hwalls;  // host copy of the wall table (block order)
     ~WcnsContext() {
         if (graph) cudaGraphExecDestroy(graph);
         for (int q = 0; q < 2; q++) {
@@ -573,6 +574,19 @@ static int check_errors(WcnsContext *c) {
     return 0;
 }
 
+// The Mach-dependent free-stream constants of init_inflow (PreProcess.f90:
+// 968-1113) and read_perfect_gasmodel (GasModel.f90:184-217) for one block,
+// evaluated as the context does for its common Mach number.
+static void set_block_freestream(DevBlock &d, const DevParams &P, double moo) {
+    d.moo2 = moo * moo;
+    d.moocp = moo * moo * P.gama;
+    d.poo = 1.0 / (P.gama * moo * moo);
+    d.coo = sqrt(P.gama * d.poo / P.roo);
+    const double cp = 1.0 / ((P.gama - 1.0) * moo * moo);
+    d.cp_prl = cp / 0.72;
+    d.cp_prt = cp / 0.90;
+}
+
 // ---------------------------------------------------------------------------
 extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, const double *const *xyz, int nregions,
                            const int *regions, WcnsContext **out) {
@@ -633,6 +647,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
         d.off = off;
         d.npts = (long long)d.ni * d.nj * d.nk;
         d.pmoff = c->total_pm;
+        set_block_freestream(d, P, prm->moo);
         c->total_pm += (long long)(d.ni + d.nj + d.nk - 2) * d.nj * d.nk;
         c->total_pm = (c->total_pm + 31) / 32 * 32;
         off += (long long)d.gx * d.gy * d.gz;
@@ -734,7 +749,14 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
                 for (int j = 1; j <= d.nj; j++)
                     for (int i = 1; i <= d.ni; i++)
                         tmp[gidx(d, i, j, k) - d.off] = src[(i - 1) + (size_t)d.ni * ((j - 1) + (size_t)d.nj * (k - 1))];
-            cudaMemcpy(xyzd + (size_t)q * c->total + d.off, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice);
+            if (cudaMemcpy(xyzd + (size_t)q * c->total + d.off, tmp.data(), sizeof(double) * tmp.size(),
+                           cudaMemcpyHostToDevice) != cudaSuccess) {
+                set_err("wcns_create: copy of the coordinates to the device failed");
+                cudaFree(xyzd);
+                cudaFree(work);
+                delete c;
+                return WCNS_ERR_CUDA;
+            }
         }
     }
     double *xyzp[3] = {xyzd, xyzd + c->total, xyzd + 2 * c->total};
@@ -763,6 +785,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
                 W.s_lr = R.s_lr;
                 W.pt_off = npt;
                 W.quad_off = nq;
+                W.nquad = nqr;
                 const int ni = c->blk[b].d.ni, nj = c->blk[b].d.nj;
                 for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
                     for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
@@ -776,6 +799,7 @@ extern "C" int wcns_create(const WcnsParams *prm, int nblocks, const int *dims, 
             }
         L.nwall = (int)walls.size();
         L.nwall_quads = nq;
+        c->hwalls = walls;
         if (L.nwall) {
             L.walls = c->up(walls);
             L.wall_xyz = c->up(wxyz);
@@ -1042,8 +1066,21 @@ extern "C" int wcns_sa_setup(WcnsContext *c, const double *const *xyz, double ti
         c->graph = nullptr;
     }
     c->launches = 0;
-    // coordinates in the pool's layout and the wall point list
+    // coordinates in the pool's layout and the wall point list, grouped by
+    // the sets of blocks joined through interfaces (one case each): a block
+    // measures its distance to its own set's walls, as
+    // calc_wall_dists_parallel does for the one case it runs
+    std::vector<int> comp(nbk);
+    for (int b = 0; b < nbk; b++) comp[b] = b;
+    auto root = [&](int b) {
+        while (comp[b] != b) b = comp[b] = comp[comp[b]];
+        return b;
+    };
+    for (int b = 0; b < nbk; b++)
+        for (const HReg &R : c->blk[b].regs)
+            if (R.bctype < 0) comp[root(b)] = root(R.nbt - 1);
     std::vector<double> wall, tmp;
+    std::vector<int> wrange(2 * nbk, 0);
     double *xyzd = nullptr, *walld = nullptr;
     CK(cudaMalloc(&xyzd, sizeof(double) * 3 * (size_t)c->total));
     for (int b = 0; b < nbk; b++) {
@@ -1055,30 +1092,51 @@ extern "C" int wcns_sa_setup(WcnsContext *c, const double *const *xyz, double ti
                 for (int j = 1; j <= d.nj; j++)
                     for (int i = 1; i <= d.ni; i++)
                         tmp[gidx(d, i, j, k) - d.off] = src[(i - 1) + (size_t)d.ni * ((j - 1) + (size_t)d.nj * (k - 1))];
-            cudaMemcpy(xyzd + (size_t)q * c->total + d.off, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice);
-        }
-        for (const HReg &R : c->blk[b].regs) {
-            if (!(R.bctype == 2 || R.bctype == 20 || R.bctype == 21)) continue;
-            for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
-                for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
-                    for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
-                        size_t g = (size_t)(i - 1) + (size_t)d.ni * ((size_t)(j - 1) + (size_t)d.nj * (k - 1));
-                        for (int q = 0; q < 3; q++) wall.push_back(xyz[3 * b + q][g]);
-                    }
+            cudaError_t e = cudaMemcpy(xyzd + (size_t)q * c->total + d.off, tmp.data(), sizeof(double) * tmp.size(),
+                                       cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { cudaFree(xyzd); set_err(std::string("wcns_sa_setup: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
         }
     }
-    if (wall.size() / 3 > 0x7fffffff) { cudaFree(xyzd); set_err("wcns_sa_setup: too many wall points"); return WCNS_ERR_ARGUMENT; }
-    if (!wall.empty()) {
-        cudaError_t e = cudaMalloc(&walld, sizeof(double) * wall.size());
-        if (e == cudaSuccess) e = cudaMemcpy(walld, wall.data(), sizeof(double) * wall.size(), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) { cudaFree(xyzd); cudaFree(walld); set_err(std::string("wcns_sa_setup: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
+    for (int r = 0; r < nbk; r++) {
+        if (root(r) != r) continue;
+        const int w0 = (int)(wall.size() / 3);
+        for (int b = 0; b < nbk; b++) {
+            if (root(b) != r) continue;
+            const DevBlock &d = c->blk[b].d;
+            for (const HReg &R : c->blk[b].regs) {
+                if (!(R.bctype == 2 || R.bctype == 20 || R.bctype == 21)) continue;
+                for (int k = R.s_st[2]; k <= R.s_ed[2]; k++)
+                    for (int j = R.s_st[1]; j <= R.s_ed[1]; j++)
+                        for (int i = R.s_st[0]; i <= R.s_ed[0]; i++) {
+                            size_t g = (size_t)(i - 1) + (size_t)d.ni * ((size_t)(j - 1) + (size_t)d.nj * (k - 1));
+                            for (int q = 0; q < 3; q++) wall.push_back(xyz[3 * b + q][g]);
+                        }
+            }
+        }
+        if (wall.size() / 3 > 0x7fffffff) { cudaFree(xyzd); set_err("wcns_sa_setup: too many wall points"); return WCNS_ERR_ARGUMENT; }
+        const int w1 = (int)(wall.size() / 3);
+        for (int b = 0; b < nbk; b++)
+            if (root(b) == r) { wrange[2 * b] = w0; wrange[2 * b + 1] = w1; }
+    }
+    int *wranged = nullptr;
+    {
+        cudaError_t e = cudaMalloc(&wranged, sizeof(int) * wrange.size());
+        if (e == cudaSuccess) e = cudaMemcpy(wranged, wrange.data(), sizeof(int) * wrange.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !wall.empty()) e = cudaMalloc(&walld, sizeof(double) * wall.size());
+        if (e == cudaSuccess && !wall.empty()) e = cudaMemcpy(walld, wall.data(), sizeof(double) * wall.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(xyzd); cudaFree(walld); cudaFree(wranged);
+            set_err(std::string("wcns_sa_setup: ") + cudaGetErrorString(e));
+            return WCNS_ERR_CUDA;
+        }
     }
     // init_SA: vt = muoo * fv1(muoo)
     const double muoo = 1.0e-1, kf3 = pow(muoo, 3.0), vt = muoo * (kf3 / (kf3 + S.cv13));
-    launch_sa_setup(c->L, xyzd, walld, (int)(wall.size() / 3), vt);
+    launch_sa_setup(c->L, xyzd, walld, wranged, vt);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(xyzd);
+    cudaFree(wranged);
     if (walld) cudaFree(walld);
     if (e != cudaSuccess) { set_err(std::string("wcns_sa_setup: ") + cudaGetErrorString(e)); return WCNS_ERR_CUDA; }
     return 0;
@@ -1126,13 +1184,40 @@ extern "C" int wcns_residual(WcnsContext *c, double *res, double *resmax, double
     return 0;
 }
 
-// force (PostProcess.f90:1415-1480): integrate, then normalise on the host
-// as the reference does after its MPI_REDUCE
-extern "C" int wcns_forces(WcnsContext *c, const double *ref, double *out) {
-    if (!c || !ref || !out) { set_err("wcns_forces: invalid argument"); return WCNS_ERR_ARGUMENT; }
+// A block's free stream at its own Mach number, for contexts holding
+// independent cases of different Mach numbers (every other parameter is the
+// context's); the kernels read the block table on the device at run time, so
+// a captured step graph needs no rebuild.
+extern "C" int wcns_set_block_freestream(WcnsContext *c, int nb, double moo) {
+    if (!c || nb < 1 || nb > (int)c->blk.size() || !(moo > 0.0)) {
+        set_err("wcns_set_block_freestream: invalid argument");
+        return WCNS_ERR_ARGUMENT;
+    }
+    DevBlock &d = c->blk[nb - 1].d;
+    set_block_freestream(d, c->P, moo);
+    const_cast<DevBlock *>(c->L.hblocks)[nb - 1] = d;
+    CK(cudaMemcpyAsync(c->L.blocks + (nb - 1), &d, sizeof(DevBlock), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+// force (PostProcess.f90:1415-1480): integrate over the wall quads of blocks
+// nb0..nb1, then normalise on the host as the reference does after its
+// MPI_REDUCE
+static int forces_range(WcnsContext *c, int nb0, int nb1, const double *ref, double *out) {
+    if (!c || !ref || !out || nb0 < 1 || nb1 < nb0 || nb1 > (int)c->blk.size()) {
+        set_err("wcns_forces: invalid argument");
+        return WCNS_ERR_ARGUMENT;
+    }
     double cf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (c->L.nwall) {
-        launch_forces(c->L, ref[2], ref[3], ref[4]);
+    long long q0 = -1, q1 = 0;
+    for (const DevWall &W : c->hwalls)
+        if (W.blk >= nb0 - 1 && W.blk <= nb1 - 1) {
+            if (q0 < 0) q0 = W.quad_off;
+            q1 = W.quad_off + W.nquad;
+        }
+    if (c->L.nwall && q0 >= 0) {
+        launch_forces(c->L, ref[2], ref[3], ref[4], q0, q1);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(cf, c->L.wall_out, sizeof cf, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
@@ -1148,6 +1233,15 @@ extern "C" int wcns_forces(WcnsContext *c, const double *ref, double *out) {
     out[7] = cosb * (out[1] * sina + out[0] * cosa) + sinb * out[2];
     out[8] = copysign(1.0, out[1]) * out[5] / (fabs(out[1]) + SMALL);
     return 0;
+}
+
+extern "C" int wcns_forces(WcnsContext *c, const double *ref, double *out) {
+    if (!c) { set_err("wcns_forces: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    return forces_range(c, 1, (int)c->blk.size(), ref, out);
+}
+
+extern "C" int wcns_forces_blocks(WcnsContext *c, int nb0, int nb1, const double *ref, double *out) {
+    return forces_range(c, nb0, nb1, ref, out);
 }
 
 // one complete step (Main.f90:85-109) on the context stream

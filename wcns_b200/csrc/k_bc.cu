@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                 long long tI = f - sL;
                 double rin = rr[tI], uin = uu[tI], vin = vv[tI], win = ww[tI], pin = pp[tI];
                 double s_in = pin / pow(rin, gama);
-                double s_oo = P.poo / pow(P.roo, gama);
+                double s_oo = B.poo / pow(P.roo, gama);
                 double cin = sqrt(gama * pin / rin);
                 double cg = fmax(sqrt(nx * nx + ny * ny + nz * nz), SML_SSS);
                 double cgm1 = (double)R.s_lr / cg;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                 double rb, ub, vb, wb, pb;
                 if (mach < 1.0) {
                     double rp = vnin + 2.0 * cin / (gama - 1.0);
-                    double rn = vnoo - 2.0 * P.coo / (gama - 1.0);
+                    double rn = vnoo - 2.0 * B.coo / (gama - 1.0);
                     double vnb = 0.5 * (rp + rn);
                     double ab = 0.25 * (gama - 1.0) * (rp - rn);
                     double sb, uref, vref, wref, vnref;
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                 } else if (vnin > 0.0) {
                     rb = rin; ub = uin; vb = vin; wb = win; pb = pin;
                 } else {
-                    rb = P.roo; ub = P.uoo; vb = P.voo; wb = P.woo; pb = P.poo;
+                    rb = P.roo; ub = P.uoo; vb = P.voo; wb = P.woo; pb = B.poo;
                 }
                 set5(F, f, rb, ub, vb, wb, pb);
                 if (qke) {
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                 break;
             }
             case 5: {  // supersonic inflow
-                for (int n = 0; n <= 3; n++) set5(F, f + n * sL, P.roo, P.uoo, P.voo, P.woo, P.poo);
+                for (int n = 0; n <= 3; n++) set5(F, f + n * sL, P.roo, P.uoo, P.voo, P.woo, B.poo);
                 if (qke) qke[f] = qke[f + sL] = SA_MUOO_BC;
                 break;
             }
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(512) k_bc_physical(DevParams P, DevFields F, c
                         if (pres < PMIN_LIMIT) pres = pp[t1];
                         tres = P.twall_nd;
                     }
-                    double dres = P.moocp * pres / tres;
+                    double dres = B.moocp * pres / tres;
                     set5(F, f, dres, 0.0, 0.0, 0.0, pres);
                     set5(F, f + 2 * sL, rr[t2], -uu[t2], -vv[t2], -ww[t2], pp[t2]);
                     set5(F, f + 3 * sL, -rr[t3], -uu[t3], -vv[t3], -ww[t3], pp[t3]);

@@ -41,7 +41,7 @@ __global__ void k_wall_points(DevParams P, DevFields F, const DevBlock *__restri
         nx = nx / s1;
         ny = ny / s1;
         nz = nz / s1;
-        double pn = 2.0 * (F.f[F_P][id] - P.poo);
+        double pn = 2.0 * (F.f[F_P][id] - B.poo);
         const double slr = (double)Wr.s_lr;
         double fx = slr * nx * pn, fy = slr * ny * pn, fz = slr * nz * pn;
         if (P.nvis == 1) {
@@ -151,19 +151,21 @@ __global__ void k_wall_quads(const DevWall *__restrict__ walls, const double *__
     }
 }
 
-__global__ void k_wall_sum(const double *__restrict__ quad, long long nquad, double *out) {
+// sums over the quads q0..q1-1 (the walls of a range of blocks are a
+// contiguous range of quads)
+__global__ void k_wall_sum(const double *__restrict__ quad, long long q0, long long q1, double *out) {
     const int m = threadIdx.x;
     if (m >= 6) return;
     double s = 0.0;
-    for (long long q = 0; q < nquad; q++) s = s + quad[6 * q + m];
+    for (long long q = q0; q < q1; q++) s = s + quad[6 * q + m];
     out[m] = s;
 }
 
-void launch_forces(const LaunchCtx &c, double xref, double yref, double zref) {
+void launch_forces(const LaunchCtx &c, double xref, double yref, double zref, long long q0, long long q1) {
     if (c.nwall == 0) return;
     k_wall_points<<<dim3(16, c.nwall), 256, 0, c.stream>>>(*c.P, *c.F, c.blocks, c.walls, c.wall_pf);
     k_wall_quads<<<dim3(16, c.nwall), 256, 0, c.stream>>>(c.walls, c.wall_pf, c.wall_xyz, xref, yref, zref, c.wall_quad);
-    k_wall_sum<<<1, 32, 0, c.stream>>>(c.wall_quad, c.nwall_quads, c.wall_out);
+    k_wall_sum<<<1, 32, 0, c.stream>>>(c.wall_quad, q0, q1, c.wall_out);
 }
 
 }  // namespace wcns

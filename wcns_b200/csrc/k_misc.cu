@@ -26,7 +26,7 @@ __device__ __forceinline__ void decode(const DevBlock &B, long long p, int &i, i
 // ghost layers of the faces the point sits on)
 __device__ __forceinline__ void init_point(const DevParams &P, DevFields &F, const DevBlock &B, int i, int j, int k,
                                            long long id) {
-    const double gama = P.gama, moo2 = P.moo2;
+    const double gama = P.gama, moo2 = B.moo2;
     double *r = F.f[F_R], *p = F.f[F_P], *t = F.f[F_T];
 #pragma unroll
     for (int m = 0; m < 5; m++) F.f[F_DQ1 + m][id] = 0.0;

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(VIS_THREADS, 2) k_rhs_vis(DevParams P, DevFiel
             const double mu = inner ? sutherland(P, v[VS_U + 3]) : 0.0;
             const double vt = (inner && F.f[F_VIST]) ? __ldg(F.f[F_VIST] + gi) : 0.0;
             v[VS_V1] = inner ? mu + vt : 0.0;
-            v[VS_V2] = inner ? mu * P.cp_prl + vt * P.cp_prt : 0.0;
+            v[VS_V2] = inner ? mu * B.cp_prl + vt * B.cp_prt : 0.0;
             double *S = smem + (size_t)ln * LS + p;
 #pragma unroll
             for (int f = 0; f < VIS_NF; f++) S[f * W] = v[f];

@@ -268,11 +268,15 @@ __global__ void __launch_bounds__(1024) k_sa_lusgs(DevFields F, SaFields S, cons
 // the nearest wall point (exact minimum, so the order of the wall list does
 // not matter), then sqrt + small, at points 1..n.
 constexpr int WD_TILE = 512;
+// The wall points a block measures to are those of its own set of blocks
+// joined through interfaces (wall_range[2b] .. wall_range[2b+1]): one case,
+// also when independent cases share a context.
 __global__ void __launch_bounds__(256) k_sa_wall_dist(SaFields S, const double *__restrict__ xyz, long long total,
-                                                      const double *__restrict__ wall, int nwall,
+                                                      const double *__restrict__ wall, const int *__restrict__ wall_range,
                                                       const DevBlock *__restrict__ blocks) {
     __shared__ double sw[3 * WD_TILE];
     const DevBlock B = blocks[blockIdx.y];
+    const int wbeg = wall_range[2 * blockIdx.y], nwall = wall_range[2 * blockIdx.y + 1];
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool act = q < B.npts;
     long long id = 0;
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(256) k_sa_wall_dist(SaFields S, const double *
         yc = xyz[total + id];
         zc = xyz[2 * total + id];
     }
-    for (int w0 = 0; w0 < nwall; w0 += WD_TILE) {
+    for (int w0 = wbeg; w0 < nwall; w0 += WD_TILE) {
         const int nt = nwall - w0 < WD_TILE ? nwall - w0 : WD_TILE;
         __syncthreads();
         for (int e = threadIdx.x; e < 3 * nt; e += blockDim.x) sw[e] = wall[3 * (long long)w0 + e];
@@ -331,10 +335,10 @@ unsigned grid_for(long long n) {
 
 }  // namespace
 
-void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, int nwall, double vt) {
+void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, const int *wall_range, double vt) {
     k_sa_init<<<dim3(grid_for(max_points(c, 3)), c.nblocks), 256, 0, c.stream>>>(*c.SA, vt, c.blocks);
     k_sa_wall_dist<<<dim3((unsigned)((max_points(c, 0) + 255) / 256), c.nblocks), 256, 0, c.stream>>>(
-        *c.SA, xyz, c.total, wall, nwall, c.blocks);
+        *c.SA, xyz, c.total, wall, wall_range, c.blocks);
 }
 
 int launch_turbulence(const LaunchCtx &c) {

@@ -61,6 +61,11 @@ struct DevBlock {
     long long off;   // base offset of this block in every field
     long long npts;  // ni*nj*nk
     long long pmoff; // base offset in the plane-major sweep arrays
+    // the free stream's Mach-dependent constants of init_inflow
+    // (PreProcess.f90:968-1113) for this block: the context's by default,
+    // a case's own when independent cases of different Mach numbers share
+    // one context (wcns_set_block_freestream)
+    double moo2, moocp, poo, coo, cp_prl, cp_prt;
 };
 
 // Plane-major layout for the LU-SGS sweeps.  Cell (i,j,k) of a block lives

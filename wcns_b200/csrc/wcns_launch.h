@@ -51,6 +51,7 @@ struct DevWall {
     int s_st[3], e[3], s_lr3d[3], s_lr;
     long long pt_off;    // first point in the wall point arrays
     long long quad_off;  // first quad in the quad array
+    long long nquad;     // quads of the region
 };
 
 // Spalart-Allmaras model arrays (one field each, the pool's layout): qke,
@@ -230,13 +231,14 @@ int setup_sweep(LaunchCtx &c, int cluster, int fine);
 // the sweeps' bounded wait on an mbarrier nothing completes (self-test)
 void launch_wait_probe(const LaunchCtx &c, long long limit);
 void launch_update(const LaunchCtx &c);
-void launch_forces(const LaunchCtx &c, double xref, double yref, double zref);
+void launch_forces(const LaunchCtx &c, double xref, double yref, double zref, long long q0, long long q1);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
 int setup_residual(int nblocks, int ctas);  // -1 when the block count is too large
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
 // SA model: set-up (init_SA and the wall distance; xyz: 3 fields of the
 // pool's layout, wall: 3 doubles per wall point) and one model step
-void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, int nwall, double vt);
+// wall_range: per block the [begin, end) of its set's wall points (device)
+void launch_sa_setup(const LaunchCtx &c, const double *xyz, const double *wall, const int *wall_range, double vt);
 int launch_turbulence(const LaunchCtx &c);  // returns the number of launches
 
 }  // namespace wcns

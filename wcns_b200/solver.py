@@ -64,6 +64,9 @@ class Wcns:
                              regs.ctypes.data_as(C.POINTER(C.c_int)), C.byref(h)))
         self.h = h
         self._xyz = (keep, xyz_p)
+        if getattr(case, "block_moo", None):
+            for nb, m in enumerate(case.block_moo, start=1):
+                self.set_block_freestream(nb, m)
         for nb, prim in enumerate(case.prim, start=1):
             self.set_prim(nb, prim)
 
@@ -260,6 +263,17 @@ class Wcns:
         out = np.zeros(9)
         _check(_lib.load().wcns_forces(self.h, ref.ctypes.data, out.ctypes.data))
         return dict(zip(FORCE_KEYS, out))
+
+    def force_blocks(self, nb0, nb1, sref=1.0, lfref=1.0, xref=0.0, yref=0.0, zref=0.0, nwholefield=1):
+        """Force coefficients over the walls of blocks nb0..nb1 (one case of a batch)."""
+        ref = np.array([sref, lfref, xref, yref, zref, nwholefield], dtype=np.float64)
+        out = np.zeros(9)
+        _check(_lib.load().wcns_forces_blocks(self.h, nb0, nb1, ref.ctypes.data, out.ctypes.data))
+        return dict(zip(FORCE_KEYS, out))
+
+    def set_block_freestream(self, nb, moo):
+        """Block nb's free stream at Mach moo (a case of a batch)."""
+        _check(_lib.load().wcns_set_block_freestream(self.h, nb, moo))
 
     def step(self, nsteps=1, history=True):
         """nsteps whole time steps (Main.f90:79-127) replayed from a CUDA graph."""
