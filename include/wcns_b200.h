@@ -208,6 +208,17 @@ int wcns_n_multipoints(WcnsContext *ctx);
  * block cluster per block), 1 one launch per hyperplane, 2 wide cooperative
  * sweeps (see WCNS_FLAG_SWEEP_BY_PLANE and WCNS_FLAG_SWEEP_WIDE). */
 int wcns_sweep_mode(WcnsContext *ctx);
+/* Arithmetic of the residual (r_h_s_vis and r_h_s_invis): 64 (default) the
+ * FP64 restatement of the reference's operation order; 32 mixed precision,
+ * with FP32 interpolation, fluxes, viscous derivatives and stresses while
+ * the metrics, the smoothness indicators' denominators and the accumulation
+ * into dq stay FP64.  The time step, the SA model, the LU-SGS sweeps and the
+ * update are FP64 in both.  A precision change drops the captured step graph
+ * (it is captured again at the next wcns_step).  Returns WCNS_ERR_ARGUMENT
+ * for any other value. */
+int wcns_set_precision(WcnsContext *ctx, int bits);
+/* 64 or 32, as set by wcns_set_precision. */
+int wcns_get_precision(WcnsContext *ctx);
 /* Failure-path self-test: runs the LU-SGS sweep's bounded wait (every wait
  * of the sweep kernels gives up after a clock-cycle limit instead of hanging)
  * on an mbarrier that nothing completes, with a limit of limit_cycles

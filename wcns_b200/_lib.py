@@ -50,6 +50,8 @@ SIGNATURES = {
     "wcns_launches_per_step": (C.c_int, [_VP]),
     "wcns_n_multipoints": (C.c_int, [_VP]),
     "wcns_sweep_mode": (C.c_int, [_VP]),
+    "wcns_set_precision": (C.c_int, [_VP, C.c_int]),
+    "wcns_get_precision": (C.c_int, [_VP]),
     "wcns_selftest_timeout": (C.c_int, [_VP, C.c_longlong]),
     "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
     "wcns_forces_blocks": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),

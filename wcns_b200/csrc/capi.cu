@@ -468,25 +468,29 @@ static int build_tables(WcnsContext *c) {
         L.mem_idx = c->up(wr_idx);
         L.blk_mem_first = c->up(blk_wr_first);
     }
-    // line groups for the residual kernels
-    size_t inv_smem = 0, vis_smem = 0;
+    // line groups for the residual kernels (passes 2 and 3: the mixed-precision ones)
+    size_t inv_smem = 0, vis_smem = 0, inv_mx_smem = 0, vis_mx_smem = 0;
     for (int dir = 0; dir < 3; dir++) {
-        for (int pass = 0; pass < 2; pass++) {  // 0 inviscid, 1 viscous
+        for (int pass = 0; pass < 4; pass++) {  // 0 inviscid, 1 viscous, 2 and 3 the same in mixed precision
             std::vector<LineGroup> g;
             int nl_max = 0, hmax = 0;
             size_t sm_dir = 0;
             for (int b = 0; b < nbk; b++) {
                 const DevBlock &D = c->blk[b].d;
                 int n = dimof(D, dir);
-                if (pass == 0 && n <= NIJK2D) continue;
+                if ((pass == 0 || pass == 2) && n <= NIJK2D) continue;
                 int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
                 int na = dimof(D, a1), nb2 = dimof(D, a2);
-                size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : rhs_vis_line_bytes(n);
+                size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : pass == 1 ? rhs_vis_line_bytes(n)
+                                : pass == 2 ? rhs_invis_mx_line_bytes(n) : rhs_vis_mx_line_bytes(n);
                 // at most 72 KB of staged lines per CTA: three 256-thread inviscid or two
-                // 384-thread viscous CTAs per SM (both kernels are bounded to 80 registers)
+                // 384-thread viscous CTAs per SM (all four kernels are bounded to 80 registers)
                 int NL = pass == 0 ? std::max(1, std::min({rhs_invis_max_lines(), 3072 / (5 * (n + 2)),
                                                            (int)((72 * 1024) / per_line)}))
-                                   : std::max(1, std::min({rhs_vis_max_lines(), 512 / (n + 1), (int)((72 * 1024) / per_line)}));
+                       : pass == 1 ? std::max(1, std::min({rhs_vis_max_lines(), 512 / (n + 1), (int)((72 * 1024) / per_line)}))
+                       : pass == 2 ? std::max(1, std::min({rhs_invis_mx_max_lines(), 3072 / (5 * (n + 2)),
+                                                           (int)((72 * 1024) / per_line)}))
+                                   : std::max(1, std::min({rhs_vis_mx_max_lines(), 512 / (n + 1), (int)((72 * 1024) / per_line)}));
                 for (int bb = 1; bb <= nb2; bb++)
                     for (int a = 1; a <= na; a += NL) {
                         LineGroup lg{b, a, bb, std::min(NL, na - a + 1)};
@@ -496,20 +500,22 @@ static int build_tables(WcnsContext *c) {
                     }
                 hmax = std::max(hmax, n + 1);
             }
-            DirTable &T = pass == 0 ? L.inv[dir] : L.vis[dir];
+            DirTable &T = pass == 0 ? L.inv[dir] : pass == 1 ? L.vis[dir] : pass == 2 ? L.inv_mx[dir] : L.vis_mx[dir];
             T.ngroups = (int)g.size();
             T.nl_max = nl_max;
             T.hmax = hmax;
             T.smem = sm_dir;
             T.groups = c->up(g);
             size_t sm = sm_dir;
-            if (pass == 0) inv_smem = std::max(inv_smem, sm);
-            else vis_smem = std::max(vis_smem, sm);
+            size_t &acc = pass == 0 ? inv_smem : pass == 1 ? vis_smem : pass == 2 ? inv_mx_smem : vis_mx_smem;
+            acc = std::max(acc, sm);
         }
     }
     if (inv_smem > 227 * 1024 || vis_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
     setup_rhs_invis_attrs(std::max<size_t>(inv_smem, 48 * 1024));
     setup_rhs_vis_attrs(std::max<size_t>(vis_smem, 48 * 1024));
+    if (inv_mx_smem > 227 * 1024 || vis_mx_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
+    setup_rhs_mx_attrs(std::max<size_t>(inv_mx_smem, 48 * 1024), std::max<size_t>(vis_mx_smem, 48 * 1024));
     // LU-SGS sweep shape; WCNS_SWEEP_CLUSTER (CTAs per block) and WCNS_SWEEP_FINE (0: three
     // threads per column) override it for tuning
     {
@@ -1386,6 +1392,30 @@ extern "C" int wcns_launches_per_step(WcnsContext *c) {
     return c->launches;
 }
 extern "C" int wcns_n_multipoints(WcnsContext *c) { return c ? c->nmulti : 0; }
+// 64: the residual in FP64 with the reference's operation order (default);
+// 32: the mixed-precision residual of k_rhs_mixed.cu.  The rest of the step
+// is FP64 either way.
+extern "C" int wcns_set_precision(WcnsContext *c, int bits) {
+    if (!c) { set_err("wcns_set_precision: null context"); return WCNS_ERR_ARGUMENT; }
+    if (bits != 64 && bits != 32) { set_err("wcns_set_precision: bits must be 64 or 32"); return WCNS_ERR_ARGUMENT; }
+    const int mixed = bits == 32 ? 1 : 0;
+    if (mixed != c->L.mixed) {
+        CK(cudaStreamSynchronize(c->stream));
+        c->L.mixed = mixed;
+        c->L.duv32 = (float *)c->F.f[F_DUV0];  // the FP64 node derivatives are unused meanwhile
+        if (c->graph) {  // the captured step holds the other kernels
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
+    return 0;
+}
+
+extern "C" int wcns_get_precision(WcnsContext *c) {
+    if (!c) return -1;
+    return c->L.mixed ? 32 : 64;
+}
+
 extern "C" int wcns_sweep_mode(WcnsContext *c) {
     if (!c) return -1;
     return c->L.wide ? 2 : c->L.sweep_plane ? 1 : 0;

@@ -334,7 +334,7 @@ __global__ void k_combine_dq(DevFields F, const DevBlock *__restrict__ blocks, c
 }
 
 void launch_rhs_dirs(const LaunchCtx &c, bool vis) {
-    const DirTable *T = vis ? c.vis : c.inv;
+    const DirTable *T = c.mixed ? (vis ? c.vis_mx : c.inv_mx) : (vis ? c.vis : c.inv);
     double *out[3] = {nullptr, c.contrib, c.contrib + 5 * c.total};
     const bool has[3] = {T[0].ngroups > 0, T[1].ngroups > 0, T[2].ngroups > 0};
     cudaEventRecord(c.ev_fork, c.stream);

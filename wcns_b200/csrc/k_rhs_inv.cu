@@ -376,6 +376,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, 
 }
 
 void launch_rhs_invis(const LaunchCtx &c, int dir, cudaStream_t st, double *out) {
+    if (c.mixed) return launch_rhs_invis_mx(c, dir, st, out);
     const DirTable &T = c.inv[dir];
     if (T.ngroups == 0) return;
     const long long stride = c.total;

@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(256, 4) k_node_deriv(DevParams P, DevFields F,
 }
 
 void launch_node_derivatives(const LaunchCtx &c) {
+    if (c.mixed) return launch_node_derivatives_mx(c);
     long long maxp = 0;
     for (int b = 0; b < c.nblocks; b++) maxp = c.hblocks[b].npts > maxp ? c.hblocks[b].npts : maxp;
     int gx = (int)((maxp + 255) / 256);
@@ -294,6 +295,7 @@ size_t rhs_vis_line_bytes(int n) { return (size_t)vis_line_stride(n) * 8; }
 int rhs_vis_max_lines() { return VIS_MAX_LINES; }
 
 void launch_rhs_vis(const LaunchCtx &c, int dir, cudaStream_t st, double *out) {
+    if (c.mixed) return launch_rhs_vis_mx(c, dir, st, out);
     const DirTable &T = c.vis[dir];
     if (T.ngroups == 0) return;
     const long long stride = c.total;

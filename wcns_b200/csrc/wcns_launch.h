@@ -122,6 +122,12 @@ struct LaunchCtx {
     int nblocks = 0;
     int *err = nullptr;            // device error slots
     DirTable inv[3], vis[3];
+    // mixed precision (wcns_set_precision(ctx, 32)): the residual kernels of
+    // k_rhs_mixed.cu with their own line groups, and FP32 node derivatives
+    // of (u,v,w,T) in the storage of the FP64 ones (12 x total floats)
+    int mixed = 0;
+    DirTable inv_mx[3], vis_mx[3];
+    float *duv32 = nullptr;
     // boundary conditions
     GhostCopy *ghost = nullptr;
     long long nghost = 0;
@@ -217,6 +223,15 @@ void launch_rhs_dirs(const LaunchCtx &c, bool vis);
 void setup_rhs_vis_attrs(size_t max_smem);
 size_t rhs_vis_line_bytes(int n);  // shared memory of one line in k_rhs_vis
 int rhs_vis_max_lines();           // lines per CTA in k_rhs_vis
+// mixed-precision residual (k_rhs_mixed.cu)
+void launch_rhs_invis_mx(const LaunchCtx &c, int dir, cudaStream_t st, double *out);
+void launch_rhs_vis_mx(const LaunchCtx &c, int dir, cudaStream_t st, double *out);
+void launch_node_derivatives_mx(const LaunchCtx &c);
+void setup_rhs_mx_attrs(size_t inv_smem, size_t vis_smem);
+size_t rhs_invis_mx_line_bytes(int n);
+size_t rhs_vis_mx_line_bytes(int n);
+int rhs_invis_mx_max_lines();
+int rhs_vis_mx_max_lines();
 void launch_boundary(const LaunchCtx &c);
 void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);

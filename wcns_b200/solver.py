@@ -303,5 +303,15 @@ class Wcns:
         """How the LU-SGS sweeps run: "clustered", "plane" or "wide"."""
         return ("clustered", "plane", "wide")[int(_lib.load().wcns_sweep_mode(self.h))]
 
+    def set_precision(self, bits: int):
+        """64: the FP64 residual (default); 32: the mixed-precision residual
+        (FP32 interpolation, fluxes and viscous arithmetic; FP64 metrics,
+        smoothness-indicator denominators, dq accumulation and LU-SGS)."""
+        _check(_lib.load().wcns_set_precision(self.h, int(bits)))
+
+    @property
+    def precision(self) -> int:
+        return int(_lib.load().wcns_get_precision(self.h))
+
     def n_multipoints(self) -> int:
         return int(_lib.load().wcns_n_multipoints(self.h))
