@@ -19,6 +19,14 @@ Prints one JSON line.  Metric: Mcell-steps/s = points x steps / seconds.
             copied in from pinned host memory (wcns_set_interior, flow-file
             layout), the step runs (wcns_step), the same fields are copied
             back (wcns_get_interior) and the residual read (wcns_residual).
+  mixed_precision -- (one GPU) the same workload with the mixed-precision
+            residual (wcns_set_precision 32): Mcell-steps/s, speed-up over
+            the FP64 line, per-variable relative L2 and wall-force errors
+            against a fresh FP64 context after the same steps.
+  batch64 -- (one GPU) 64 independent small SA bump cases: every case on
+            its own FP64 context one after another, all in one FP64
+            context, all in one context with the mixed-precision residual;
+            Mcell-steps/s of each, speed-ups, errors of the mixed batch.
   --impl reference -- the CPU restatement of the reference path (the oracle;
             the Fortran reference cannot be built here) on all host cores,
             same workload and config.
@@ -62,6 +70,9 @@ def parse():
     ap.add_argument("--case", default="channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-tune", action="store_true", help="run the default launch shapes (no autotuner)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the mixed-precision and 64-case batch measurements")
     return ap.parse_args()
 
 
@@ -300,15 +311,176 @@ def profile_phases(g, reps=3):
     return out
 
 
+def timed_steps(g, steps, stream, flush=None):
+    """Device ms of `steps` graph replays on the context's stream (back to
+    back, or one by one after an L2 flush when `flush` is given)."""
+    import torch
+    torch.cuda.synchronize()
+    if flush is None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step_async(steps)
+        e1.record(stream)
+        g.sync()
+        return e0.elapsed_time(e1)
+    evs = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        g.step_async(1)
+        b.record(stream)
+        evs.append((a, b))
+    g.sync()
+    return sum(a.elapsed_time(b) for a, b in evs)
+
+
+def rel_l2(a_ctx, b_ctx, names, dims, blocks_a=None, blocks_b=None):
+    """Relative L2 (over the interior points) of every field of `names`:
+    context a against context b, block lists matched in order."""
+    import numpy as np
+    ba = blocks_a or list(range(1, len(dims) + 1))
+    bb = blocks_b or ba
+    out = {}
+    for name in names:
+        num = den = 0.0
+        for x, y in zip(ba, bb):
+            ni, nj, nk = dims[y - 1]
+            a = a_ctx.get(name, x)[3:3 + nk, 3:3 + nj, 3:3 + ni]
+            b = b_ctx.get(name, y)[3:3 + nk, 3:3 + nj, 3:3 + ni]
+            num += float(np.sum((a - b) ** 2))
+            den += float(np.sum(b * b))
+        out[name] = float((num / den) ** 0.5) if den > 0 else float(num ** 0.5)
+    return out
+
+
+def measure_mixed(case, value64, steps, warmup, tune=True):
+    """The same workload with the mixed-precision residual: Mcell-steps/s,
+    speed-up over the FP64 line and, after `warmup + steps` steps from the
+    same start, the error of every variable and wall-force coefficient
+    against a fresh FP64 context (the FP64 path equals the oracle to 1e-12)."""
+    import torch
+    from wcns_b200.solver import Wcns
+    from wcns_b200 import autotune
+    g = Wcns(case)
+    sa_prepare(g, case)
+    g.set_precision(32)
+    shape = autotune.tuned(g)["shape"] if tune else g.shape
+    stream = torch.cuda.ExternalStream(g.stream)
+    g.step(warmup, history=False)
+    ms = timed_steps(g, steps, stream)
+    value = case.npoints * steps / (ms / 1e3) / 1e6
+    ref = Wcns(case)
+    sa_prepare(ref, case)
+    ref.step(warmup + steps, history=False)
+    names = ["r", "u", "v", "w", "p"] + (["qke"] if case.sa else [])
+    err = rel_l2(g, ref, names, case.dims)
+    fg, fr = g.force(), ref.force()
+    g.close()
+    ref.close()
+    return {"value": round(value, 4), "unit": METRIC, "ms_per_step": round(ms / steps, 4),
+            "speedup_vs_fp64": round(value / value64, 4), "shape": shape,
+            "dtype": "f32 residual arithmetic; f64 metrics, IS denominators, dq sum, SA, LU-SGS, update",
+            "after_steps": warmup + steps,
+            "rel_l2_vs_fp64": {k: float(f"{v:.3e}") for k, v in err.items()},
+            "force_rel_err_vs_fp64": force_errors(fg, fr)}
+
+
+def force_errors(f, ref):
+    """Errors of the wall-force coefficients cfx, cfy: each relative to its
+    own value, and relative to the largest of |cfx|, |cfy|, |cfz| (a
+    coefficient that is the small net of two walls' forces has no scale of
+    its own)."""
+    big = max(abs(ref[k]) for k in ("cfx", "cfy", "cfz"))
+    out = {}
+    for k in ("cfx", "cfy"):
+        d = abs(f[k] - ref[k])
+        out[k] = float(f"{d / max(abs(ref[k]), 1e-300):.3e}")
+        out[k + "_vs_largest"] = float(f"{d / max(big, 1e-300):.3e}")
+    out["values"] = {k: float(f"{ref[k]:.6e}") for k in ("cfx", "cfy")}
+    return out
+
+
+def measure_batch(steps, warmup, ncases=64, tune=True):
+    """C4's batch: 64 independent small SA bump cases (block sizes 17^3 ..
+    49x33x17, Mach U[0.3,0.8], bump U[0.02,0.08], seed 0).  Three forms, each
+    `steps` steps after `warmup`, device-timed: every case on its own FP64
+    context one after another (the plain per-case path), all cases in one
+    FP64 context, and all cases in one context with the mixed-precision
+    residual; then the errors of the mixed batch against the plain per-case
+    runs (per-variable relative L2, the worst case's wall-force error)."""
+    import torch
+    from wcns_b200 import autotune, cases
+    from wcns_b200.solver import Wcns
+    b = cases.batch_case(ncases=ncases, seed=0)
+    npts = b.npoints
+    members = [cases.batch_member(b, q) for q in range(ncases)]
+    sep_ms, singles = 0.0, []
+    for m in members:
+        h = Wcns(m)
+        sa_prepare(h, m)
+        if tune:
+            autotune.tuned(h)
+        h.step(warmup, history=False)
+        sep_ms += timed_steps(h, steps, torch.cuda.ExternalStream(h.stream))
+        singles.append(h)
+    res = {"cases": ncases, "points": npts, "steps": steps,
+           "fp64_separate": {"value": round(npts * steps / (sep_ms / 1e3) / 1e6, 4), "ms_per_step": round(sep_ms / steps, 4),
+                      "note": "every case on its own context, one after another" + (", each autotuned" if tune else "")}}
+    batched = {}
+    for bits in (64, 32):
+        g = Wcns(b)
+        sa_prepare(g, b)
+        g.set_precision(bits)
+        if tune:
+            autotune.tuned(g)
+        g.step(warmup, history=False)
+        ms = timed_steps(g, steps, torch.cuda.ExternalStream(g.stream))
+        res[f"fp{bits}_batched"] = {"value": round(npts * steps / (ms / 1e3) / 1e6, 4), "ms_per_step": round(ms / steps, 4),
+                                    "shape": g.shape}
+        batched[bits] = g
+    g = batched[32]
+    names = ["r", "u", "v", "w", "p", "qke"]
+    num = {k: 0.0 for k in names}
+    den = {k: 0.0 for k in names}
+    worst = {"cfx": 0.0, "cfy": 0.0, "cfx_vs_largest": 0.0, "cfy_vs_largest": 0.0}
+    for q, h in enumerate(singles):
+        nb0, _ = b.groups[q]
+        e = rel_l2(g, h, names, members[q].dims, [nb0], [1])
+        for k in names:  # pool the squared norms over the cases
+            import numpy as np
+            ni, nj, nk = members[q].dims[0]
+            bref = h.get(k, 1)[3:3 + nk, 3:3 + nj, 3:3 + ni]
+            d2 = float(np.sum(bref * bref))
+            num[k] += (e[k] ** 2) * d2
+            den[k] += d2
+        fe = force_errors(g.force_blocks(nb0, nb0), h.force())
+        for k in worst:
+            worst[k] = max(worst[k], fe[k])
+    for h in singles:
+        h.close()
+    for g in batched.values():
+        g.close()
+    sep = res["fp64_separate"]["value"]
+    res["speedup_fp32_batched_vs_fp64_separate"] = round(res["fp32_batched"]["value"] / sep, 3)
+    res["speedup_fp32_batched_vs_fp64_batched"] = round(res["fp32_batched"]["value"] / res["fp64_batched"]["value"], 3)
+    res["fp32_batched_rel_l2_vs_fp64_separate"] = {k: float(f"{(num[k] / den[k]) ** 0.5:.3e}") for k in names}
+    res["fp32_batched_worst_case_force_rel_err"] = {k: float(f"{v:.3e}") for k, v in worst.items()}
+    return res
+
+
 def run_b200(args, rank, world):
     import numpy as np
     import torch
 
+    from wcns_b200 import autotune
     from wcns_b200.solver import Wcns
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     case = make_case(args.case)
     g = Wcns(case)
     sa_prepare(g, case)
+    tune = autotune.tuned(g) if not args.no_tune else {"shape": g.shape, "source": "default"}
     stream = torch.cuda.ExternalStream(g.stream)
     big = case_resident_bytes(case) > 4 * L2_BYTES
     flush = None if big else torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -400,6 +572,12 @@ def run_b200(args, rank, world):
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {e}"}
+    sweep_mode, launches = g.sweep_mode(), g.launches_per_step()
+    g.close()
+    mixed = batch = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        mixed = measure_mixed(case, value, args.steps, args.warmup, not args.no_tune)
+        batch = measure_batch(args.steps, args.warmup, tune=not args.no_tune)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world,
@@ -418,13 +596,16 @@ def run_b200(args, rank, world):
                          "sweeps": {"share": round(sum(e["share"] for e in sweeps), 4),
                                     "ms": round(sum(e["ms"] for e in sweeps), 4)}},
             "phases": ph,
-            "sweep_mode": g.sweep_mode(),
-            "gpu_launches": g.launches_per_step() * args.steps,
+            "sweep_mode": sweep_mode,
+            "autotune": tune,
+            "gpu_launches": launches * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
         }
+        if mixed is not None:
+            line["mixed_precision"] = mixed
+            line["batch64"] = batch
         print(json.dumps(line), flush=True)
-    g.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

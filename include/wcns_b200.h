@@ -219,6 +219,26 @@ int wcns_sweep_mode(WcnsContext *ctx);
 int wcns_set_precision(WcnsContext *ctx, int bits);
 /* 64 or 32, as set by wcns_set_precision. */
 int wcns_get_precision(WcnsContext *ctx);
+/* Launch shapes: shape[0] CTAs per block cluster of the clustered LU-SGS
+ * sweeps (0 when the context sweeps wide or by plane), shape[1] 1 for
+ * sixteen lanes per (j,k) column, 0 for three, shape[2] / shape[3] lines per
+ * CTA of the inviscid / viscous residual kernels at most (1..32).  No shape
+ * changes a result.  wcns_set_shape returns WCNS_ERR_ARGUMENT for a shape the
+ * blocks cannot run (the shape in use stays); it drops the captured step
+ * graph. */
+int wcns_get_shape(WcnsContext *ctx, int *shape);
+/* The context device's name, compute capability and SM count (for keying
+ * cached shapes), NUL-terminated in buf[len]. */
+int wcns_device_name(WcnsContext *ctx, char *buf, int len);
+int wcns_set_shape(WcnsContext *ctx, const int *shape);
+/* Autotuner: times every candidate shape (clusters of 1, 2, 4, 8, 16 CTAs in
+ * both lane modes; 4, 8, 16, 32 lines per CTA for each residual kernel) on
+ * the context's current state, reps timed runs each after one warm-up, with
+ * the phase each shapes (the LU-SGS phase; the inviscid and the viscous
+ * residual), keeps the fastest and returns it in shape[4]; ms[3] (may be
+ * NULL) receives the best device ms of those three phases.  The state is
+ * not changed (dq is restored).  Takes a few hundred phase runs. */
+int wcns_autotune(WcnsContext *ctx, int reps, int *shape, double *ms);
 /* Failure-path self-test: runs the LU-SGS sweep's bounded wait (every wait
  * of the sweep kernels gives up after a clock-cycle limit instead of hanging)
  * on an mbarrier that nothing completes, with a limit of limit_cycles

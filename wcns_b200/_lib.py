@@ -52,6 +52,10 @@ SIGNATURES = {
     "wcns_sweep_mode": (C.c_int, [_VP]),
     "wcns_set_precision": (C.c_int, [_VP, C.c_int]),
     "wcns_get_precision": (C.c_int, [_VP]),
+    "wcns_get_shape": (C.c_int, [_VP, _VP]),
+    "wcns_device_name": (C.c_int, [_VP, C.c_char_p, C.c_int]),
+    "wcns_set_shape": (C.c_int, [_VP, _VP]),
+    "wcns_autotune": (C.c_int, [_VP, C.c_int, _VP, _VP]),
     "wcns_selftest_timeout": (C.c_int, [_VP, C.c_longlong]),
     "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
     "wcns_forces_blocks": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),

@@ -242,6 +242,68 @@ static int analyze(WcnsContext *c) {
 }
 
 // ---------------------------------------------------------------------------
+// Line groups of the residual kernels for every direction (passes 2 and 3:
+// the mixed-precision kernels): at most inv_cap / vis_cap lines of a block
+// per CTA, fewer where the staged lines would pass 72 KB of shared memory.
+static int build_line_tables(WcnsContext *c, int inv_cap, int vis_cap) {
+    LaunchCtx &L = c->L;
+    const int nbk = (int)c->blk.size();
+    size_t inv_smem = 0, vis_smem = 0, inv_mx_smem = 0, vis_mx_smem = 0;
+    for (int dir = 0; dir < 3; dir++) {
+        for (int pass = 0; pass < 4; pass++) {  // 0 inviscid, 1 viscous, 2 and 3 the same in mixed precision
+            std::vector<LineGroup> g;
+            int nl_max = 0, hmax = 0;
+            size_t sm_dir = 0;
+            for (int b = 0; b < nbk; b++) {
+                const DevBlock &D = c->blk[b].d;
+                int n = dimof(D, dir);
+                if ((pass == 0 || pass == 2) && n <= NIJK2D) continue;
+                int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
+                int na = dimof(D, a1), nb2 = dimof(D, a2);
+                size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : pass == 1 ? rhs_vis_line_bytes(n)
+                                : pass == 2 ? rhs_invis_mx_line_bytes(n) : rhs_vis_mx_line_bytes(n);
+                // at most 72 KB of staged lines per CTA: three 256-thread inviscid or two
+                // 384-thread viscous CTAs per SM (all four kernels are bounded to 80 registers)
+                int NL = pass == 0 ? std::max(1, std::min({std::min(inv_cap, rhs_invis_max_lines()), 3072 / (5 * (n + 2)),
+                                                           (int)((72 * 1024) / per_line)}))
+                       : pass == 1 ? std::max(1, std::min({std::min(vis_cap, rhs_vis_max_lines()), 512 / (n + 1), (int)((72 * 1024) / per_line)}))
+                       : pass == 2 ? std::max(1, std::min({std::min(inv_cap, rhs_invis_mx_max_lines()), 3072 / (5 * (n + 2)),
+                                                           (int)((72 * 1024) / per_line)}))
+                                   : std::max(1, std::min({std::min(vis_cap, rhs_vis_mx_max_lines()), 512 / (n + 1), (int)((72 * 1024) / per_line)}));
+                for (int bb = 1; bb <= nb2; bb++)
+                    for (int a = 1; a <= na; a += NL) {
+                        LineGroup lg{b, a, bb, std::min(NL, na - a + 1)};
+                        g.push_back(lg);
+                        nl_max = std::max(nl_max, lg.nl);
+                        sm_dir = std::max(sm_dir, per_line * lg.nl);
+                    }
+                hmax = std::max(hmax, n + 1);
+            }
+            DirTable &T = pass == 0 ? L.inv[dir] : pass == 1 ? L.vis[dir] : pass == 2 ? L.inv_mx[dir] : L.vis_mx[dir];
+            T.ngroups = (int)g.size();
+            T.nl_max = nl_max;
+            T.hmax = hmax;
+            T.smem = sm_dir;
+            if (T.groups) {  // a rebuild (wcns_set_shape): the old table goes
+                c->owned.erase(std::remove(c->owned.begin(), c->owned.end(), (void *)T.groups), c->owned.end());
+                cudaFree(T.groups);
+            }
+            T.groups = c->up(g);
+            size_t sm = sm_dir;
+            size_t &acc = pass == 0 ? inv_smem : pass == 1 ? vis_smem : pass == 2 ? inv_mx_smem : vis_mx_smem;
+            acc = std::max(acc, sm);
+        }
+    }
+    if (inv_smem > 227 * 1024 || vis_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
+    setup_rhs_invis_attrs(std::max<size_t>(inv_smem, 48 * 1024));
+    setup_rhs_vis_attrs(std::max<size_t>(vis_smem, 48 * 1024));
+    if (inv_mx_smem > 227 * 1024 || vis_mx_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
+    setup_rhs_mx_attrs(std::max<size_t>(inv_mx_smem, 48 * 1024), std::max<size_t>(vis_mx_smem, 48 * 1024));
+    L.inv_cap = inv_cap;
+    L.vis_cap = vis_cap;
+    return 0;
+}
+
 static int build_tables(WcnsContext *c) {
     const int nbk = (int)c->blk.size();
     LaunchCtx &L = c->L;
@@ -468,54 +530,7 @@ static int build_tables(WcnsContext *c) {
         L.mem_idx = c->up(wr_idx);
         L.blk_mem_first = c->up(blk_wr_first);
     }
-    // line groups for the residual kernels (passes 2 and 3: the mixed-precision ones)
-    size_t inv_smem = 0, vis_smem = 0, inv_mx_smem = 0, vis_mx_smem = 0;
-    for (int dir = 0; dir < 3; dir++) {
-        for (int pass = 0; pass < 4; pass++) {  // 0 inviscid, 1 viscous, 2 and 3 the same in mixed precision
-            std::vector<LineGroup> g;
-            int nl_max = 0, hmax = 0;
-            size_t sm_dir = 0;
-            for (int b = 0; b < nbk; b++) {
-                const DevBlock &D = c->blk[b].d;
-                int n = dimof(D, dir);
-                if ((pass == 0 || pass == 2) && n <= NIJK2D) continue;
-                int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
-                int na = dimof(D, a1), nb2 = dimof(D, a2);
-                size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : pass == 1 ? rhs_vis_line_bytes(n)
-                                : pass == 2 ? rhs_invis_mx_line_bytes(n) : rhs_vis_mx_line_bytes(n);
-                // at most 72 KB of staged lines per CTA: three 256-thread inviscid or two
-                // 384-thread viscous CTAs per SM (all four kernels are bounded to 80 registers)
-                int NL = pass == 0 ? std::max(1, std::min({rhs_invis_max_lines(), 3072 / (5 * (n + 2)),
-                                                           (int)((72 * 1024) / per_line)}))
-                       : pass == 1 ? std::max(1, std::min({rhs_vis_max_lines(), 512 / (n + 1), (int)((72 * 1024) / per_line)}))
-                       : pass == 2 ? std::max(1, std::min({rhs_invis_mx_max_lines(), 3072 / (5 * (n + 2)),
-                                                           (int)((72 * 1024) / per_line)}))
-                                   : std::max(1, std::min({rhs_vis_mx_max_lines(), 512 / (n + 1), (int)((72 * 1024) / per_line)}));
-                for (int bb = 1; bb <= nb2; bb++)
-                    for (int a = 1; a <= na; a += NL) {
-                        LineGroup lg{b, a, bb, std::min(NL, na - a + 1)};
-                        g.push_back(lg);
-                        nl_max = std::max(nl_max, lg.nl);
-                        sm_dir = std::max(sm_dir, per_line * lg.nl);
-                    }
-                hmax = std::max(hmax, n + 1);
-            }
-            DirTable &T = pass == 0 ? L.inv[dir] : pass == 1 ? L.vis[dir] : pass == 2 ? L.inv_mx[dir] : L.vis_mx[dir];
-            T.ngroups = (int)g.size();
-            T.nl_max = nl_max;
-            T.hmax = hmax;
-            T.smem = sm_dir;
-            T.groups = c->up(g);
-            size_t sm = sm_dir;
-            size_t &acc = pass == 0 ? inv_smem : pass == 1 ? vis_smem : pass == 2 ? inv_mx_smem : vis_mx_smem;
-            acc = std::max(acc, sm);
-        }
-    }
-    if (inv_smem > 227 * 1024 || vis_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
-    setup_rhs_invis_attrs(std::max<size_t>(inv_smem, 48 * 1024));
-    setup_rhs_vis_attrs(std::max<size_t>(vis_smem, 48 * 1024));
-    if (inv_mx_smem > 227 * 1024 || vis_mx_smem > 227 * 1024) { set_err("line too long for shared memory"); return WCNS_ERR_ARGUMENT; }
-    setup_rhs_mx_attrs(std::max<size_t>(inv_mx_smem, 48 * 1024), std::max<size_t>(vis_mx_smem, 48 * 1024));
+    if (int rc = build_line_tables(c, INV_LINES_DEFAULT, VIS_LINES_DEFAULT)) return rc;
     // LU-SGS sweep shape; WCNS_SWEEP_CLUSTER (CTAs per block) and WCNS_SWEEP_FINE (0: three
     // threads per column) override it for tuning
     {
@@ -1414,6 +1429,155 @@ extern "C" int wcns_set_precision(WcnsContext *c, int bits) {
 extern "C" int wcns_get_precision(WcnsContext *c) {
     if (!c) return -1;
     return c->L.mixed ? 32 : 64;
+}
+
+// ---------------------------------------------------------------------------
+// Launch shapes and their autotuner.  shape[0]: CTAs per block cluster of the
+// clustered LU-SGS sweeps (0 when the sweeps run wide or by plane);
+// shape[1]: 1 sixteen lanes per column, 0 three; shape[2], shape[3]: lines
+// per CTA of the inviscid / viscous residual kernels at most.  No shape
+// changes a result: every point's arithmetic is the same in each.
+
+static bool clustered_sweeps(const WcnsContext *c) { return !c->L.wide && !c->L.sweep_plane; }
+
+static void drop_graph(WcnsContext *c) {
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+}
+
+// name of the context's device (for keying tuned shapes), NUL-terminated in buf[len]
+extern "C" int wcns_device_name(WcnsContext *c, char *buf, int len) {
+    if (!c || !buf || len < 1) { set_err("wcns_device_name: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    int dev = 0;
+    cudaDeviceProp prop;
+    CK(cudaGetDevice(&dev));
+    CK(cudaGetDeviceProperties(&prop, dev));
+    snprintf(buf, (size_t)len, "%s sm_%d%d %d SMs", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+    return 0;
+}
+
+extern "C" int wcns_get_shape(WcnsContext *c, int *shape) {
+    if (!c || !shape) { set_err("wcns_get_shape: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    shape[0] = clustered_sweeps(c) ? c->L.sweep_cluster : 0;
+    shape[1] = clustered_sweeps(c) ? c->L.sweep_fine : 0;
+    shape[2] = c->L.inv_cap;
+    shape[3] = c->L.vis_cap;
+    return 0;
+}
+
+static int apply_shape(WcnsContext *c, const int *shape) {
+    LaunchCtx &L = c->L;
+    if (clustered_sweeps(c) && (shape[0] != L.sweep_cluster || shape[1] != L.sweep_fine)) {
+        if (setup_sweep_exact(L, shape[0], shape[1])) {
+            set_err("wcns_set_shape: the blocks cannot be swept with " + std::to_string(shape[0]) +
+                    " CTAs per cluster in that lane mode");
+            return WCNS_ERR_ARGUMENT;
+        }
+        c->PM.csize = L.sweep_cluster;
+    }
+    if (shape[2] != L.inv_cap || shape[3] != L.vis_cap)
+        if (int rc = build_line_tables(c, shape[2], shape[3])) return rc;
+    drop_graph(c);
+    return 0;
+}
+
+extern "C" int wcns_set_shape(WcnsContext *c, const int *shape) {
+    if (!c || !shape) { set_err("wcns_set_shape: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    if (shape[2] < 1 || shape[2] > INV_LINES_DEFAULT || shape[3] < 1 || shape[3] > VIS_LINES_DEFAULT) {
+        set_err("wcns_set_shape: lines per CTA must be in 1..32");
+        return WCNS_ERR_ARGUMENT;
+    }
+    if (clustered_sweeps(c) && (shape[0] < 1 || shape[1] < 0 || shape[1] > 1)) {
+        set_err("wcns_set_shape: the clustered sweeps need shape[0] >= 1 and shape[1] in 0..1");
+        return WCNS_ERR_ARGUMENT;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return apply_shape(c, shape);
+}
+
+// Device ms of `reps` runs of `body` on the context stream, dq restored from
+// `saved` before each (outside the timed interval).
+template <class Body>
+static double time_reps(WcnsContext *c, int reps, const double *saved, Body body) {
+    double *dq = c->F.f[F_DQ1];
+    const size_t bytes = sizeof(double) * 5 * (size_t)c->total;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double total = 0.0;
+    for (int r = 0; r <= reps; r++) {  // the first run is a warm-up
+        cudaMemcpyAsync(dq, saved, bytes, cudaMemcpyDeviceToDevice, c->stream);
+        cudaEventRecord(e0, c->stream);
+        body();
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0) total += ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return total / reps;
+}
+
+// Times every candidate shape on the context's current state with the
+// phases it shapes (the LU-SGS phase for the sweep shape, the inviscid and
+// viscous residual for the line caps), keeps the fastest, and returns it in
+// shape[4]; ms[3] (may be NULL) receives the best device ms of the three
+// phases.  The state (prim, SA fields) is not changed; dq is restored.
+extern "C" int wcns_autotune(WcnsContext *c, int reps, int *shape, double *ms) {
+    if (!c || !shape || reps < 1) { set_err("wcns_autotune: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    LaunchCtx &L = c->L;
+    CK(cudaStreamSynchronize(c->stream));
+    double *saved = nullptr;
+    const size_t bytes = sizeof(double) * 5 * (size_t)c->total;
+    CK(cudaMalloc(&saved, bytes));
+    CK(cudaMemcpy(saved, c->F.f[F_DQ1], bytes, cudaMemcpyDeviceToDevice));
+    int best[4];
+    wcns_get_shape(c, best);
+    double best_ms[3] = {0.0, 0.0, 0.0};
+    // the LU-SGS sweep shape
+    if (clustered_sweeps(c)) {
+        double tbest = 1e300;
+        const int cls[5] = {1, 2, 4, 8, 16};
+        for (int fine = 1; fine >= 0; fine--)
+            for (int q = 0; q < 5; q++) {
+                int cand[4] = {cls[q], fine, best[2], best[3]};
+                if (setup_sweep_exact(L, cand[0], cand[1])) continue;
+                c->PM.csize = L.sweep_cluster;
+                const double t = time_reps(c, reps, saved, [&] { launch_lhs(L); });
+                if (t < tbest) { tbest = t; best[0] = cand[0]; best[1] = cand[1]; }
+            }
+        setup_sweep_exact(L, best[0], best[1]);
+        c->PM.csize = L.sweep_cluster;
+        best_ms[0] = tbest;
+    }
+    // lines per CTA of the residual kernels
+    const int caps[4] = {4, 8, 16, 32};
+    for (int vis = 0; vis <= (c->P.nvis == 1 ? 1 : 0); vis++) {
+        if (vis) launch_node_derivatives(L);
+        double tbest = 1e300;
+        int kbest = vis ? best[3] : best[2];
+        for (int q = 0; q < 4; q++) {
+            const int ic = vis ? best[2] : caps[q], vc = vis ? caps[q] : best[3];
+            if (build_line_tables(c, ic, vc)) continue;
+            const double t = time_reps(c, reps, saved, [&] { launch_rhs_dirs(L, vis == 1); });
+            if (t < tbest) { tbest = t; kbest = caps[q]; }
+        }
+        best[vis ? 3 : 2] = kbest;
+        best_ms[vis ? 2 : 1] = tbest;
+        build_line_tables(c, best[2], best[3]);
+    }
+    cudaMemcpy(c->F.f[F_DQ1], saved, bytes, cudaMemcpyDeviceToDevice);
+    cudaFree(saved);
+    drop_graph(c);
+    CK(cudaGetLastError());
+    for (int q = 0; q < 4; q++) shape[q] = best[q];
+    if (ms)
+        for (int q = 0; q < 3; q++) ms[q] = best_ms[q];
+    return check_errors(c);
 }
 
 extern "C" int wcns_sweep_mode(WcnsContext *c) {

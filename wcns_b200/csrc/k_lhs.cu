@@ -689,6 +689,26 @@ int setup_sweep(LaunchCtx &c, int cluster, int fine) {
     return -1;
 }
 
+// Exactly the shape (cl CTAs per block cluster, sixteen lanes per column
+// when fine, else three); -1 when the blocks cannot be swept with it, with
+// the shape in use left as it was.
+int setup_sweep_exact(LaunchCtx &c, int cl, int fine) {
+    int maxnj = 0, maxnk = 0, minnj = 1 << 30;
+    for (int b = 0; b < c.nblocks; b++) {
+        maxnj = std::max(maxnj, c.hblocks[b].nj);
+        maxnk = std::max(maxnk, c.hblocks[b].nk);
+        minnj = std::min(minnj, c.hblocks[b].nj);
+    }
+    if (cl < 1 || cl > 16 || cl > minnj) return -1;
+    const int cpc = (maxnj + cl - 1) / cl * maxnk;
+    const int old_cl = c.sweep_cluster, old_cpc = c.sweep_cpc, old_fine = c.sweep_fine;
+    if (fine ? try_sweep_shape<true>(c, cl, cpc) : try_sweep_shape<false>(c, cl, cpc)) return 0;
+    // a refused shape may have changed the kernels' shared-memory attributes
+    if (old_fine) try_sweep_shape<true>(c, old_cl, old_cpc);
+    else try_sweep_shape<false>(c, old_cl, old_cpc);
+    return -1;
+}
+
 int launch_lhs(const LaunchCtx &c) {
     const int zg = (int)((c.nzero + 255) / 256);
     if (c.wide) {

@@ -126,6 +126,9 @@ struct LaunchCtx {
     // k_rhs_mixed.cu with their own line groups, and FP32 node derivatives
     // of (u,v,w,T) in the storage of the FP64 ones (12 x total floats)
     int mixed = 0;
+    // lines per CTA of the inviscid / viscous residual kernels at most (the
+    // tunable pencil tile, wcns_set_shape / wcns_autotune)
+    int inv_cap = 32, vis_cap = 32;
     DirTable inv_mx[3], vis_mx[3];
     float *duv32 = nullptr;
     // boundary conditions
@@ -243,6 +246,8 @@ int setup_sweep_wide(LaunchCtx &c, WideSweep &W);  // -1: the blocks cannot be s
 int launch_sweeps_wide(const LaunchCtx &c);
 int launch_sa_lusgs_wide(const LaunchCtx &c);  // needs wide->A.sa
 int setup_sweep(LaunchCtx &c, int cluster, int fine);
+int setup_sweep_exact(LaunchCtx &c, int cluster, int fine);  // -1: not valid for the blocks
+constexpr int INV_LINES_DEFAULT = 32, VIS_LINES_DEFAULT = 32;
 // the sweeps' bounded wait on an mbarrier nothing completes (self-test)
 void launch_wait_probe(const LaunchCtx &c, long long limit);
 void launch_update(const LaunchCtx &c);

@@ -48,6 +48,8 @@ class Wcns:
     def __init__(self, case, flags=0):
         L = _lib.load()
         self.case = case
+        self.flags = int(flags)
+        self.sa_ready = False
         self.dims = [tuple(int(v) for v in d) for d in case.dims]
         self._prm = params_struct(case.params, flags)
         dims = (C.c_int * (3 * len(self.dims)))(*[v for d in self.dims for v in d])
@@ -245,6 +247,7 @@ class Wcns:
         """Model arrays, wall distance (calc_wall_dists_parallel) and init_SA;
         fields "qke", "vist", "dist" become readable and writable."""
         _check(_lib.load().wcns_sa_setup(self.h, self._xyz[1], timedt_turb, kmaxlim))
+        self.sa_ready = True
 
     def turbulence(self):
         """turbulence(nb) for every block (RHS.f90:22)."""
@@ -312,6 +315,33 @@ class Wcns:
     @property
     def precision(self) -> int:
         return int(_lib.load().wcns_get_precision(self.h))
+
+    @property
+    def shape(self) -> list:
+        """[cluster CTAs of the sweeps (0: wide or by plane), fine lanes,
+        inviscid lines per CTA, viscous lines per CTA]."""
+        out = np.zeros(4, dtype=np.int32)
+        _check(_lib.load().wcns_get_shape(self.h, out.ctypes.data))
+        return [int(v) for v in out]
+
+    def device_name(self) -> str:
+        buf = C.create_string_buffer(256)
+        _check(_lib.load().wcns_device_name(self.h, buf, 256))
+        return buf.value.decode()
+
+    def set_shape(self, shape):
+        arr = np.ascontiguousarray(shape, dtype=np.int32)
+        if arr.shape != (4,):
+            raise ValueError("a shape has four entries")
+        _check(_lib.load().wcns_set_shape(self.h, arr.ctypes.data))
+
+    def autotune(self, reps=3):
+        """Times the candidate shapes on the current state and keeps the
+        fastest: (shape, best ms of the LU-SGS, inviscid and viscous phases)."""
+        out = np.zeros(4, dtype=np.int32)
+        ms = np.zeros(3)
+        _check(_lib.load().wcns_autotune(self.h, int(reps), out.ctypes.data, ms.ctypes.data))
+        return [int(v) for v in out], [float(v) for v in ms]
 
     def n_multipoints(self) -> int:
         return int(_lib.load().wcns_n_multipoints(self.h))
