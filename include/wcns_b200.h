@@ -239,6 +239,49 @@ int wcns_set_shape(WcnsContext *ctx, const int *shape);
  * NULL) receives the best device ms of those three phases.  The state is
  * not changed (dq is restored).  Takes a few hundred phase runs. */
 int wcns_autotune(WcnsContext *ctx, int reps, int *shape, double *ms);
+
+/* Tangent and adjoint of the inviscid residual and of the LU-SGS operator
+ * (inviscid contexts with nscheme 4 and the Steger-Warming or Roe flux;
+ * other contexts return WCNS_ERR_UNSUPPORTED).  The operands live in slots
+ * of the context, five fields each in the ghosted layout of wcns_set_prim
+ * (allocated on first use): */
+#define WCNS_ADJ_V 0     /* tangent input: a prim-space direction (ghosts included) */
+#define WCNS_ADJ_RDOT 1  /* tangent output: (dr/dq) v at the interior points */
+#define WCNS_ADJ_LAM 2   /* adjoint input: lambda at the interior points */
+#define WCNS_ADJ_QBAR 3  /* adjoint output: (dr/dq)^T lambda in prim space, ghosts included */
+#define WCNS_ADJ_B 4     /* LU-SGS operator input */
+#define WCNS_ADJ_X 5     /* LU-SGS operator output */
+#define WCNS_ADJ_G 6     /* adjoint iteration: dJ/dQ, the objective's gradient in conserved variables */
+#define WCNS_ADJ_PSI 7   /* adjoint iteration: the adjoint state (conserved variables) */
+#define WCNS_ADJ_W 8     /* work */
+#define WCNS_ADJ_NSLOTS 9
+/* r is the inviscid residual of wcns_rhs_invis (dq of r_h_s_invis,
+ * RHS.f90:35-72) as a function of the ghosted prim q, linearised at the
+ * context's current state (run wcns_boundary_all first, and
+ * wcns_initial_q_dq_c_t and wcns_timestep before the LU-SGS operator). */
+int wcns_adj_set(WcnsContext *ctx, int slot, int nb, const double *const *five);
+int wcns_adj_get(WcnsContext *ctx, int slot, int nb, double *const *five);
+int wcns_adj_zero(WcnsContext *ctx, int slot);
+/* forward: RDOT = (dr/dq) V */
+int wcns_rhs_invis_tangent(WcnsContext *ctx);
+/* backward: QBAR = (dr/dq)^T LAM (WCNS-E-5 transposed with its nonlinear
+ * weights recomputed, the flux Jacobian applied transposed).  fold != 0:
+ * interface ghosts are copies of partner points (exchange_bc), so their
+ * adjoint is moved to the partner point; the ghosts of physical boundaries
+ * keep their share either way (they are inputs held fixed). */
+int wcns_rhs_invis_adjoint(WcnsContext *ctx, int fold);
+/* X = P B (transpose 0) or X = P^T B (transpose 1), P the operator of one
+ * lower and one upper LU-SGS sweep (lusgs_l, lusgs_u, LHS.f90:381-577):
+ * P b = -(I + C U)^-1 (I - C L)^-1 C b over the interior points. */
+int wcns_lusgs_operator(WcnsContext *ctx, int transpose);
+/* iters steps of the adjoint fixed point psi <- psi + Z P^T Z (r_Q^T psi + g)
+ * (r_Q: the residual's Jacobian in conserved variables; Z zeroes the points
+ * of physical faces, whose dq the step zeroes before and after the sweeps),
+ * whose fixed point solves Z (r_Q^T psi + g) = 0 with psi = 0 on those
+ * faces; hist[iters] (may be NULL) receives the 2-norm of
+ * Z (r_Q^T psi + g) before each step.  Sets the ghosts, time step and spectral
+ * radii of the current state first; the state itself is not changed. */
+int wcns_adjoint_iterate(WcnsContext *ctx, int iters, double *hist);
 /* Failure-path self-test: runs the LU-SGS sweep's bounded wait (every wait
  * of the sweep kernels gives up after a clock-cycle limit instead of hanging)
  * on an mbarrier that nothing completes, with a limit of limit_cycles

@@ -56,6 +56,13 @@ SIGNATURES = {
     "wcns_device_name": (C.c_int, [_VP, C.c_char_p, C.c_int]),
     "wcns_set_shape": (C.c_int, [_VP, _VP]),
     "wcns_autotune": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "wcns_adj_set": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "wcns_adj_get": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "wcns_adj_zero": (C.c_int, [_VP, C.c_int]),
+    "wcns_rhs_invis_tangent": (C.c_int, [_VP]),
+    "wcns_rhs_invis_adjoint": (C.c_int, [_VP, C.c_int]),
+    "wcns_lusgs_operator": (C.c_int, [_VP, C.c_int]),
+    "wcns_adjoint_iterate": (C.c_int, [_VP, C.c_int, _VP]),
     "wcns_selftest_timeout": (C.c_int, [_VP, C.c_longlong]),
     "wcns_forces": (C.c_int, [_VP, _VP, _VP]),
     "wcns_forces_blocks": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),

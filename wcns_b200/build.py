@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwcns_b200.so")
-SOURCES = ["capi.cu", "k_rhs_inv.cu", "k_rhs_vis.cu", "k_bc.cu", "k_misc.cu", "k_lhs.cu", "k_metrics.cu", "k_force.cu", "noalloc.cu", "k_sa.cu", "k_sweep_plane.cu", "k_sweep_wide.cu", "k_rhs_mixed.cu"]
+SOURCES = ["capi.cu", "k_rhs_inv.cu", "k_rhs_vis.cu", "k_bc.cu", "k_misc.cu", "k_lhs.cu", "k_metrics.cu", "k_force.cu", "noalloc.cu", "k_sa.cu", "k_sweep_plane.cu", "k_sweep_wide.cu", "k_rhs_mixed.cu", "k_adjoint.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 

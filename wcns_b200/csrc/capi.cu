@@ -103,6 +103,7 @@ struct WcnsContext {
     int launches = 0;
     std::unique_ptr<WideSweep> wide;
     std::vector<DevWall> hwalls;  // host copy of the wall table (block order)
+    double *adj_pool = nullptr;   // the adjoint slots (WCNS_ADJ_*), five fields each, on first use
     ~WcnsContext() {
         if (graph) cudaGraphExecDestroy(graph);
         for (int q = 0; q < 2; q++) {
@@ -114,6 +115,7 @@ struct WcnsContext {
         if (pool) cudaFree(pool);
         if (pm_pool) cudaFree(pm_pool);
         if (sa_pool) cudaFree(sa_pool);
+        if (adj_pool) cudaFree(adj_pool);
         if (stream) cudaStreamDestroy(stream);
     }
     template <class T>
@@ -1583,4 +1585,120 @@ extern "C" int wcns_autotune(WcnsContext *c, int reps, int *shape, double *ms) {
 extern "C" int wcns_sweep_mode(WcnsContext *c) {
     if (!c) return -1;
     return c->L.wide ? 2 : c->L.sweep_plane ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Tangent / adjoint of the inviscid residual and the LU-SGS operator pair
+// (k_adjoint.cu), on five-field slots of the context (WCNS_ADJ_*).
+
+static int adj_ready(WcnsContext *c, const char *who) {
+    if (c->P.nvis != 0 || c->P.nscheme != 4 || (c->P.nflux != 1 && c->P.nflux != 3)) {
+        set_err(std::string(who) + ": the adjoint covers the inviscid residual with nscheme 4 and the Steger-Warming or Roe flux");
+        return WCNS_ERR_UNSUPPORTED;
+    }
+    if (!c->adj_pool) {
+        const size_t bytes = sizeof(double) * 5 * (size_t)WCNS_ADJ_NSLOTS * (size_t)c->total;
+        CK(cudaMalloc(&c->adj_pool, bytes));
+        CK(cudaMemset(c->adj_pool, 0, bytes));
+    }
+    return 0;
+}
+static double *adj_slot(WcnsContext *c, int s) { return c->adj_pool + (size_t)s * 5 * (size_t)c->total; }
+
+static int adj_copy(WcnsContext *c, int slot, int nb, double *const *ptrs, bool to_device, const char *who) {
+    if (int rc = adj_ready(c, who)) return rc;
+    if (slot < 0 || slot >= WCNS_ADJ_NSLOTS || !ptrs) { set_err(std::string(who) + ": invalid argument"); return WCNS_ERR_ARGUMENT; }
+    const DevBlock *d = nullptr;
+    if (int rc = block_range(c, nb, &d)) return rc;
+    const size_t n = (size_t)d->gx * d->gy * d->gz;
+    for (int m = 0; m < 5; m++) {
+        if (!ptrs[m]) { set_err(std::string(who) + ": null array"); return WCNS_ERR_ARGUMENT; }
+        double *dev = adj_slot(c, slot) + (size_t)m * c->total + d->off;
+        CK(cudaMemcpyAsync(to_device ? (void *)dev : (void *)ptrs[m], to_device ? (const void *)ptrs[m] : (const void *)dev,
+                           sizeof(double) * n, to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_adj_set(WcnsContext *c, int slot, int nb, const double *const *five) {
+    if (!c) { set_err("wcns_adj_set: null context"); return WCNS_ERR_ARGUMENT; }
+    return adj_copy(c, slot, nb, (double *const *)five, true, "wcns_adj_set");
+}
+extern "C" int wcns_adj_get(WcnsContext *c, int slot, int nb, double *const *five) {
+    if (!c) { set_err("wcns_adj_get: null context"); return WCNS_ERR_ARGUMENT; }
+    return adj_copy(c, slot, nb, five, false, "wcns_adj_get");
+}
+extern "C" int wcns_adj_zero(WcnsContext *c, int slot) {
+    if (!c) { set_err("wcns_adj_zero: null context"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = adj_ready(c, "wcns_adj_zero")) return rc;
+    if (slot < 0 || slot >= WCNS_ADJ_NSLOTS) { set_err("wcns_adj_zero: invalid slot"); return WCNS_ERR_ARGUMENT; }
+    CK(cudaMemsetAsync(adj_slot(c, slot), 0, sizeof(double) * 5 * (size_t)c->total, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_rhs_invis_tangent(WcnsContext *c) {
+    if (!c) { set_err("wcns_rhs_invis_tangent: null context"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = adj_ready(c, "wcns_rhs_invis_tangent")) return rc;
+    CK(cudaMemsetAsync(adj_slot(c, WCNS_ADJ_RDOT), 0, sizeof(double) * 5 * (size_t)c->total, c->stream));
+    launch_rhs_invis_jvp(c->L, adj_slot(c, WCNS_ADJ_V), adj_slot(c, WCNS_ADJ_RDOT));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_rhs_invis_adjoint(WcnsContext *c, int fold) {
+    if (!c) { set_err("wcns_rhs_invis_adjoint: null context"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = adj_ready(c, "wcns_rhs_invis_adjoint")) return rc;
+    CK(cudaMemsetAsync(adj_slot(c, WCNS_ADJ_QBAR), 0, sizeof(double) * 5 * (size_t)c->total, c->stream));
+    launch_rhs_invis_vjp(c->L, adj_slot(c, WCNS_ADJ_LAM), adj_slot(c, WCNS_ADJ_QBAR), fold != 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_lusgs_operator(WcnsContext *c, int transpose) {
+    if (!c) { set_err("wcns_lusgs_operator: null context"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = adj_ready(c, "wcns_lusgs_operator")) return rc;
+    launch_lusgs_operator(c->L, adj_slot(c, WCNS_ADJ_X), adj_slot(c, WCNS_ADJ_B), transpose != 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int wcns_adjoint_iterate(WcnsContext *c, int iters, double *hist) {
+    if (!c || iters < 1) { set_err("wcns_adjoint_iterate: invalid argument"); return WCNS_ERR_ARGUMENT; }
+    if (int rc = adj_ready(c, "wcns_adjoint_iterate")) return rc;
+    LaunchCtx &L = c->L;
+    // the linearisation point's ghosts, time step and spectral radii
+    launch_boundary(L);
+    launch_init_timestep(L);
+    double *t = adj_slot(c, WCNS_ADJ_W), *psi = adj_slot(c, WCNS_ADJ_PSI), *x = adj_slot(c, WCNS_ADJ_X);
+    double *nrm = nullptr;
+    CK(cudaMalloc(&nrm, sizeof(double)));
+    const size_t bytes = sizeof(double) * 5 * (size_t)c->total;
+    int rc = 0;
+    for (int it = 0; it < iters && !rc; it++) {
+        cudaMemsetAsync(t, 0, bytes, c->stream);
+        launch_rhs_invis_vjp(L, psi, t, true);                        // (dr/dq)^T psi
+        launch_adj_to_conserved(L, t, adj_slot(c, WCNS_ADJ_G));       // r_Q^T psi + g
+        launch_adj_zero_faces(L, t);                                  // the step's operator is Z P Z
+        cudaMemsetAsync(nrm, 0, sizeof(double), c->stream);
+        launch_adj_norm2(L, t, nrm);
+        launch_lusgs_operator(L, x, t, true);                         // Z P^T Z (r_Q^T psi + g)
+        launch_adj_zero_faces(L, x);
+        launch_adj_axpy(L, psi, x);
+        double h = 0.0;
+        if (cudaMemcpyAsync(&h, nrm, sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess) {
+            set_err(std::string("wcns_adjoint_iterate: ") + cudaGetErrorString(cudaGetLastError()));
+            rc = WCNS_ERR_CUDA;
+        }
+        if (hist) hist[it] = sqrt(h);
+    }
+    cudaFree(nrm);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return check_errors(c);
 }

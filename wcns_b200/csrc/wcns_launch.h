@@ -235,6 +235,15 @@ size_t rhs_invis_mx_line_bytes(int n);
 size_t rhs_vis_mx_line_bytes(int n);
 int rhs_invis_mx_max_lines();
 int rhs_vis_mx_max_lines();
+// tangent and adjoint of the inviscid residual, the LU-SGS operator pair
+// (k_adjoint.cu); x, v, lam, out, b, g: five arrays LaunchCtx::total apart
+void launch_rhs_invis_jvp(const LaunchCtx &c, const double *v, double *out);
+void launch_rhs_invis_vjp(const LaunchCtx &c, const double *lam, double *out, bool fold);
+void launch_lusgs_operator(const LaunchCtx &c, double *x, const double *b, bool transpose);
+void launch_adj_to_conserved(const LaunchCtx &c, double *x, const double *g);
+void launch_adj_axpy(const LaunchCtx &c, double *y, const double *x);
+void launch_adj_norm2(const LaunchCtx &c, const double *x, double *out);
+void launch_adj_zero_faces(const LaunchCtx &c, double *x);
 void launch_boundary(const LaunchCtx &c);
 void launch_init(const LaunchCtx &c);
 void launch_timestep(const LaunchCtx &c);

@@ -343,5 +343,46 @@ class Wcns:
         _check(_lib.load().wcns_autotune(self.h, int(reps), out.ctypes.data, ms.ctypes.data))
         return [int(v) for v in out], [float(v) for v in ms]
 
+    # ---- tangent / adjoint of the inviscid residual, LU-SGS operator pair
+    ADJ = {"v": 0, "rdot": 1, "lam": 2, "qbar": 3, "b": 4, "x": 5, "g": 6, "psi": 7, "w": 8}
+
+    def adj_set(self, slot, nb, five):
+        ni, nj, nk = self.dims[nb - 1]
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in five]
+        if len(arrs) != 5 or any(a.shape != (nk + 6, nj + 6, ni + 6) for a in arrs):
+            raise ValueError("five arrays of the block's ghosted shape")
+        ptrs = (C.c_void_p * 5)(*[a.ctypes.data for a in arrs])
+        _check(_lib.load().wcns_adj_set(self.h, self.ADJ[slot], nb, ptrs))
+
+    def adj_get(self, slot, nb):
+        ni, nj, nk = self.dims[nb - 1]
+        out = [np.empty((nk + 6, nj + 6, ni + 6)) for _ in range(5)]
+        ptrs = (C.c_void_p * 5)(*[a.ctypes.data for a in out])
+        _check(_lib.load().wcns_adj_get(self.h, self.ADJ[slot], nb, ptrs))
+        return out
+
+    def adj_zero(self, slot):
+        _check(_lib.load().wcns_adj_zero(self.h, self.ADJ[slot]))
+
+    def rhs_invis_tangent(self):
+        """rdot = (dr/dq) v at the current state (r: the inviscid residual)."""
+        _check(_lib.load().wcns_rhs_invis_tangent(self.h))
+
+    def rhs_invis_adjoint(self, fold=True):
+        """qbar = (dr/dq)^T lam at the current state; fold: interface ghosts'
+        adjoint moved to their partner points."""
+        _check(_lib.load().wcns_rhs_invis_adjoint(self.h, 1 if fold else 0))
+
+    def lusgs_operator(self, transpose=False):
+        """x = P b (or P^T b): one lower and one upper LU-SGS sweep."""
+        _check(_lib.load().wcns_lusgs_operator(self.h, 1 if transpose else 0))
+
+    def adjoint_iterate(self, iters):
+        """psi <- psi + P^T (r_Q^T psi + g), iters times; the norms of
+        r_Q^T psi + g before each step."""
+        hist = np.zeros(int(iters))
+        _check(_lib.load().wcns_adjoint_iterate(self.h, int(iters), hist.ctypes.data))
+        return hist
+
     def n_multipoints(self) -> int:
         return int(_lib.load().wcns_n_multipoints(self.h))
