@@ -131,11 +131,17 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 __device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
-// waits until *p >= want; gives up after `limit` clock cycles
-__device__ __forceinline__ bool wait_count(const unsigned *p, unsigned want, long long limit) {
+// waits until *p >= want; gives up after `limit` clock cycles.  `seen` is the
+// largest count this thread has acquired from *p so far: a count it has
+// already seen needs no new load (the acquire that saw it orders every
+// later read of the entries it covers)
+__device__ __forceinline__ bool wait_count(const unsigned *p, unsigned want, long long limit, unsigned &seen) {
+    if (seen >= want) return true;
     const long long t0 = clock64();
-    while (ld_acquire(p) < want)
+    unsigned v;
+    while ((v = ld_acquire(p)) < want)
         if (clock64() - t0 > limit) return false;
+    seen = v;
     return true;
 }
 // bring [ptr, ptr + n doubles) into L2 (the range is widened to 16-byte
@@ -270,6 +276,7 @@ __global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F
     };
     if (t == 0)
         for (int a = 0; a < WIDE_PREFETCH; a++) prefetch_plane(a);
+    unsigned seen_prod = 0, seen_cons = 0;
     for (int s = 0; s < np; s++) {
         const int p = pfirst + s * pstep;
         const int i = p - j - k;
@@ -311,8 +318,9 @@ __global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F
         }
         if (t == 0) {
             prefetch_plane(s + WIDE_PREFETCH);
-            if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit())) timed_out = true;
-            if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit())) timed_out = true;
+            if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit(), seen_prod)) timed_out = true;
+            if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit(), seen_cons))
+                timed_out = true;
         }
         __syncthreads();  // the previous plane's inbox and ring entries are complete
         if (t == 0 && (ring_out || ring_in)) {
@@ -623,16 +631,18 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields 
     auto limit = [&]() { return timed_out ? (1LL << 21) : (1LL << 31); };
     double ibuf = 0.0;
     const int pfirst = FWD ? 3 : B.ni + B.nj + B.nk, pstep = FWD ? 1 : -1;
-    auto prefetch_plane = [&](int s) {
-        if (s >= np) return;
+    const int pwarp = blockDim.x > 32 ? 32 : 0;
+    const int plane_lane = t - pwarp;
+    auto prefetch_plane = [&](int s) {  // one word array per lane of the prefetch warp
+        if (s >= np || plane_lane < 0 || plane_lane >= WSA_N) return;
         const int p = pfirst + s * pstep;
         int lo, hi;
         if (!active_slots(p, C.j0, C.w, B.ni, B.nk, lo, hi)) return;
         const long long pm0 = C.pmoff + (long long)(p - 3) * ncol + (long long)C.j0 * B.nk + lo;
-        for (int w = 0; w < WSA_N; w++) prefetch_l2(A.sa + (size_t)w * A.n + pm0, hi - lo + 1);
+        prefetch_l2(A.sa + (size_t)plane_lane * A.n + pm0, hi - lo + 1);
     };
-    if (t == 0)
-        for (int a = 0; a < WIDE_PREFETCH; a++) prefetch_plane(a);
+    for (int a = 0; a < WIDE_PREFETCH; a++) prefetch_plane(a);
+    unsigned seen_prod = 0, seen_cons = 0;
     for (int s = 0; s < np; s++) {
         const int p = pfirst + s * pstep;
         const int i = p - j - k;
@@ -649,10 +659,11 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields 
             spec = A.sa[(size_t)WSA_SPEC * A.n + pm];
             base = A.sa[(size_t)(FWD ? WSA_RHS : WSA_FWD) * A.n + pm];
         }
+        prefetch_plane(s + WIDE_PREFETCH);
         if (t == 0) {
-            prefetch_plane(s + WIDE_PREFETCH);
-            if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit())) timed_out = true;
-            if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit())) timed_out = true;
+            if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit(), seen_prod)) timed_out = true;
+            if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit(), seen_cons))
+                timed_out = true;
         }
         __syncthreads();
         if (t == 0 && (ring_out || ring_in)) {
