@@ -48,10 +48,18 @@ def test_channel_workload():
             faces[key] = int(r[7])
         assert len(faces) == 6
     assert sorted(set(case.regions[:, 7])) == [-1, 2, 3, 4]
-    # the bump lifts the lower wall at mid-length only
+    # the bump (height 0.05 H) lifts the lower wall at mid-length only: the
+    # lower-wall blocks spanning x = length/2 reach its height, those whose
+    # x range stays 1.5 H or more away from the middle stay flat
     lower = [nb for nb in range(1, 25) if any((case.regions[:, 0] == nb) & (case.regions[:, 7] == 2) & (case.regions[:, 3] == 1) & (case.regions[:, 4] == 1))]
-    ymin = min(float(case.xyz[nb - 1][1][:, 0, :].max()) for nb in lower)
-    assert 0.0 < ymin <= 0.05 + 1e-12
+    assert len(lower) == 12
+    mid = 0.5 * float(max(case.xyz[nb - 1][0].max() for nb in lower))
+    for nb in lower:
+        x, y = case.xyz[nb - 1][0][:, 0, :], case.xyz[nb - 1][1][:, 0, :]
+        if x.min() <= mid <= x.max():
+            assert abs(float(y.max()) - 0.05) < 2e-3
+        elif min(abs(float(x.min()) - mid), abs(float(x.max()) - mid)) >= 1.5:
+            assert float(y.max()) < 1e-4
 
 
 def test_plate_workload_size():

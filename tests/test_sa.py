@@ -233,14 +233,24 @@ def test_oracle_sa_channel_steps(oracle_lib):
     case = cases.small_channel_case()
     o = oracle_lib.Oracle(case)
     o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
-    v0 = o.get("vist", 1).copy()
+    v0 = [interior(o.get("vist", nb), o.dims[nb - 1]).copy() for nb in range(1, len(o.dims) + 1)]
     hist = o.step(3)
     assert np.all(np.isfinite(hist))
     for nb in range(1, len(o.dims) + 1):
         d = o.dims[nb - 1]
         for n in ("r", "u", "p", "qke", "vist"):
             assert np.all(np.isfinite(interior(o.get(n, nb), d)))
-    assert not np.array_equal(o.get("vist", 1), v0)
+    # lower-wall blocks: qke and vist vanish on the wall (BC_wall_turbulence),
+    # and the eddy viscosity at the first off-wall points grows far above its
+    # free-stream value
+    lower = [nb for nb in range(1, case.nblocks + 1)
+             if any((case.regions[:, 0] == nb) & (case.regions[:, 7] == 2) & (case.regions[:, 3] == 1) & (case.regions[:, 4] == 1))]
+    assert len(lower) == 12
+    for nb in lower:
+        d = o.dims[nb - 1]
+        q, v = interior(o.get("qke", nb), d), interior(o.get("vist", nb), d)
+        assert np.all(q[:, 0, :] == 0.0) and np.all(v[:, 0, :] == 0.0)
+        assert v[:, 1, :].mean() > 10.0 * v0[nb - 1][:, 1, :].mean()
 
 
 # --------------------------------------------------------------------------
