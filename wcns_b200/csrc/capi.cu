@@ -104,6 +104,12 @@ struct WcnsContext {
     std::unique_ptr<WideSweep> wide;
     std::vector<DevWall> hwalls;  // host copy of the wall table (block order)
     double *adj_pool = nullptr;   // the adjoint slots (WCNS_ADJ_*), five fields each, on first use
+    // staging of wcns_set_interior / wcns_get_interior: the interior points of
+    // up to stage_fields fields, contiguous per block and field; stage_first:
+    // per (field slot, block) the first element, device
+    double *stage = nullptr;
+    long long *stage_first = nullptr;
+    int stage_fields = 0;
     ~WcnsContext() {
         if (graph) cudaGraphExecDestroy(graph);
         for (int q = 0; q < 2; q++) {
@@ -116,6 +122,8 @@ struct WcnsContext {
         if (pm_pool) cudaFree(pm_pool);
         if (sa_pool) cudaFree(sa_pool);
         if (adj_pool) cudaFree(adj_pool);
+        if (stage) cudaFree(stage);
+        if (stage_first) cudaFree(stage_first);
         if (stream) cudaStreamDestroy(stream);
     }
     template <class T>
@@ -993,35 +1001,62 @@ extern "C" int wcns_get_flow(WcnsContext *c, double *const *flow) {
 // that array.  One strided copy per array, spread over the context's three
 // streams, one synchronisation.  Writing leaves every ghost point as it was:
 // boundary_all refills the ghost layers the path reads.
+// The interior points of named fields between host arrays (one per block and
+// field, flow-file order) and the field pool: every (block, field) array is
+// one contiguous copy into (or out of) a staging buffer of the context, and
+// one kernel per field scatters (gathers) between the buffer and the
+// ghosted layout, so the copies run at full link bandwidth instead of one
+// DMA row of ni points at a time.
 static int interior_copy(WcnsContext *c, int nfields, const int *fields, double *const *ptrs, bool to_device) {
     const char *fn = to_device ? "wcns_set_interior" : "wcns_get_interior";
     if (!c || nfields < 1 || !fields || !ptrs) { set_err(std::string(fn) + ": invalid argument"); return WCNS_ERR_ARGUMENT; }
     for (int q = 0; q < nfields; q++)
         if (!field_base(c, fields[q])) { set_err(std::string(fn) + ": unsupported field " + std::to_string(fields[q])); return WCNS_ERR_UNSUPPORTED; }
-    CK(cudaEventRecord(c->L.ev_fork, c->stream));
-    cudaStream_t st[3] = {c->stream, c->L.side[0], c->L.side[1]};
-    for (int q = 1; q < 3; q++) CK(cudaStreamWaitEvent(st[q], c->L.ev_fork, 0));
-    int e = 0;
     const int nbk = (int)c->blk.size();
-    for (int b = 0; b < nbk; b++) {
-        const DevBlock &d = c->blk[b].d;
+    if (nfields > c->stage_fields) {  // (re)size the staging buffer and its offset table
+        long long pts = 0;
+        for (int b = 0; b < nbk; b++) pts += c->blk[b].d.npts;
+        std::vector<long long> first((size_t)nfields * nbk);
         for (int q = 0; q < nfields; q++) {
-            double *host = ptrs[(size_t)nfields * b + q];
-            if (!host) continue;
-            cudaPitchedPtr dev = make_cudaPitchedPtr(field_base(c, fields[q]) + d.off, sizeof(double) * d.gx, d.gx, d.gy);
-            cudaPitchedPtr hp = make_cudaPitchedPtr(host, sizeof(double) * d.ni, d.ni, d.nj);
-            cudaMemcpy3DParms cp = {};
-            cp.srcPtr = to_device ? hp : dev;
-            cp.dstPtr = to_device ? dev : hp;
-            // the ghosted box (-2:n+3) starts 3 points before the interior in each direction
-            (to_device ? cp.dstPos : cp.srcPos) = make_cudaPos(sizeof(double) * 3, 3, 3);
-            cp.extent = make_cudaExtent(sizeof(double) * d.ni, d.nj, d.nk);
-            cp.kind = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
-            CK(cudaMemcpy3DAsync(&cp, st[e % 3]));
-            e++;
+            long long o = (long long)q * pts;
+            for (int b = 0; b < nbk; b++) {
+                first[(size_t)q * nbk + b] = o;
+                o += c->blk[b].d.npts;
+            }
         }
+        if (c->stage) cudaFree(c->stage);
+        if (c->stage_first) cudaFree(c->stage_first);
+        c->stage = nullptr;
+        c->stage_first = nullptr;
+        c->stage_fields = 0;
+        CK(cudaMalloc(&c->stage, sizeof(double) * (size_t)nfields * pts));
+        CK(cudaMalloc(&c->stage_first, sizeof(long long) * first.size()));
+        CK(cudaMemcpy(c->stage_first, first.data(), sizeof(long long) * first.size(), cudaMemcpyHostToDevice));
+        c->stage_fields = nfields;
     }
-    for (int q = 0; q < 3; q++) CK(cudaStreamSynchronize(st[q]));
+    long long pts = 0;
+    for (int b = 0; b < nbk; b++) pts += c->blk[b].d.npts;
+    for (int q = 0; q < nfields; q++) {
+        double *field = field_base(c, fields[q]);
+        double *stage = c->stage + (size_t)q * pts;
+        // a block without a host array keeps its values: gather them first,
+        // so that the scatter writes them back unchanged
+        bool anynull = false;
+        for (int b = 0; b < nbk; b++) anynull = anynull || !ptrs[(size_t)nfields * b + q];
+        if (!to_device || anynull) launch_interior_stage(c->L, false, c->stage_first + (size_t)q * nbk, field, c->stage);
+        long long o = 0;
+        for (int b = 0; b < nbk; b++) {
+            const size_t n = (size_t)c->blk[b].d.npts;
+            double *host = ptrs[(size_t)nfields * b + q];
+            if (host)
+                CK(cudaMemcpyAsync(to_device ? (void *)(stage + o) : (void *)host, to_device ? (const void *)host : (const void *)(stage + o),
+                                   sizeof(double) * n, to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, c->stream));
+            o += (long long)n;
+        }
+        if (to_device) launch_interior_stage(c->L, true, c->stage_first + (size_t)q * nbk, field, c->stage);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
     return 0;
 }
 

@@ -11,6 +11,8 @@
 //   communicate_dq_npp / communicate_pv_npp (parallel.f90:3020-3326).
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "wcns_dev.cuh"
 #include "wcns_launch.h"
 
@@ -362,6 +364,32 @@ int setup_residual(int nblocks, int ctas) {
     if (bytes > 200 * 1024) return -1;
     if (bytes > 48 * 1024) cudaFuncSetAttribute(k_residual_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return 0;
+}
+
+// interior points of one field between the ghosted layout and a contiguous
+// staging buffer (block b at stage[first[b] + p], p = (i-1) + ni*((j-1) + nj*(k-1)),
+// the flow-file order): TO_DEV scatters the staged values into the field,
+// otherwise the field is gathered into the buffer
+template <bool TO_DEV>
+__global__ void k_interior_stage(const DevBlock *__restrict__ blocks, const long long *__restrict__ first,
+                                 double *field, double *stage) {
+    const DevBlock B = blocks[blockIdx.y];
+    double *sb = stage + first[blockIdx.y];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < B.npts; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode(B, q, i, j, k);
+        const long long id = gidx(B, i, j, k);
+        if (TO_DEV) field[id] = sb[q];
+        else sb[q] = field[id];
+    }
+}
+
+void launch_interior_stage(const LaunchCtx &c, bool to_device, const long long *first, double *field, double *stage) {
+    long long maxp = 0;
+    for (int b = 0; b < c.nblocks; b++) maxp = c.hblocks[b].npts > maxp ? c.hblocks[b].npts : maxp;
+    const dim3 grid((unsigned)std::min<long long>((maxp + 255) / 256, 2048), c.nblocks);
+    if (to_device) k_interior_stage<true><<<grid, 256, 0, c.stream>>>(c.blocks, first, field, stage);
+    else k_interior_stage<false><<<grid, 256, 0, c.stream>>>(c.blocks, first, field, stage);
 }
 
 void launch_residual(const LaunchCtx &c, double *rms_slot) {

@@ -262,6 +262,8 @@ void launch_wait_probe(const LaunchCtx &c, long long limit);
 void launch_update(const LaunchCtx &c);
 void launch_forces(const LaunchCtx &c, double xref, double yref, double zref, long long q0, long long q1);
 void launch_residual(const LaunchCtx &c, double *rms_slot);
+// interior points of one field <-> a contiguous staging buffer (block b from first[b], device)
+void launch_interior_stage(const LaunchCtx &c, bool to_device, const long long *first, double *field, double *stage);
 int setup_residual(int nblocks, int ctas);  // -1 when the block count is too large
 void launch_metrics(const LaunchCtx &c, double *const *xyz_dev, double *work);
 // SA model: set-up (init_SA and the wall distance; xyz: 3 fields of the
