@@ -107,7 +107,36 @@ def test_invalid_shapes_are_refused():
     from wcns_b200.solver import Wcns, WcnsError
     g = Wcns(cases.small_plate_case())
     before = g.shape
-    for bad in ([0, 1, 32, 32], [1, 1, 0, 32], [1, 1, 32, 33], [64, 1, 32, 32], [1, 2, 32, 32]):
+    for bad in ([-1, 1, 32, 32], [1, 1, 0, 32], [1, 1, 32, 33], [64, 1, 32, 32], [1, 2, 32, 32]):
         with pytest.raises(WcnsError):
             g.set_shape(bad)
         assert g.shape == before
+
+
+@pytest.mark.gpu
+def test_switch_to_wide_sweeps_and_back():
+    """shape[0] = 0 sweeps a clustered-capable context with the wide
+    cooperative kernels (the same per-point arithmetic: equal to the
+    clustered steps within round-off); a cluster shape switches back and
+    reproduces the clustered steps bit for bit.  The SA model's scalar sweeps
+    follow (the reduced channel with SA)."""
+    case = cases.small_plate_case()
+    g0, h0, s0, _ = _run(case)
+    shape = g0.shape
+    g, h, s, _ = _run(case, [0, 0, 32, 32])
+    assert g.sweep_mode() == "wide" and g.shape[0] == 0
+    np.testing.assert_allclose(h, h0, rtol=1e-12, atol=0)
+    for a, b in zip(s, s0):
+        assert float(np.max(np.abs(a - b))) <= 1e-12 * max(float(np.max(np.abs(b))), 1.0)
+    g.set_shape(shape)
+    assert g.sweep_mode() == "clustered"
+    from wcns_b200.solver import Wcns
+    g2 = Wcns(case)
+    g2.set_shape([0, 0, 32, 32])
+    g2.set_shape(shape)
+    h2 = g2.step(3)
+    np.testing.assert_array_equal(h2, h0)
+    sa = cases.small_channel_case()
+    a, ha, _, _ = _run(sa)
+    b, hb, _, _ = _run(sa, [0, 0, 32, 32]) if a.shape[0] else (a, ha, None, None)
+    np.testing.assert_allclose(hb, ha, rtol=1e-11, atol=0)

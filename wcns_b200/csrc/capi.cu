@@ -252,6 +252,57 @@ static int analyze(WcnsContext *c) {
 }
 
 // ---------------------------------------------------------------------------
+static void free_owned(WcnsContext *c, void *p) {
+    if (!p) return;
+    c->owned.erase(std::remove(c->owned.begin(), c->owned.end(), p), c->owned.end());
+    cudaFree(p);
+}
+
+// The wide cooperative sweeps' chunks and arrays (and the SA model's when it
+// is set up); L.wide points to them.  -1: the blocks cannot be swept wide;
+// a CUDA error code when an allocation fails.
+static int wide_alloc(WcnsContext *c) {
+    LaunchCtx &L = c->L;
+    if (c->wide) {
+        L.wide = c->wide.get();
+        return 0;
+    }
+    auto W = std::make_unique<WideSweep>();
+    if (setup_sweep_wide(L, *W) != 0) return -1;
+    WideArrays &A = W->A;
+    const size_t words = (size_t)(WIDE_COEF_WORDS + 5 + 5 + 15 + 5) * A.n + 8;
+    CK(cudaMalloc(&A.stat, sizeof(double) * words));
+    c->owned.push_back(A.stat);
+    A.rhs = A.stat + (size_t)WIDE_COEF_WORDS * A.n;
+    A.dql = A.rhs + (size_t)5 * A.n;
+    A.gs1 = A.dql + (size_t)5 * A.n;
+    A.gs2 = A.gs1 + (size_t)15 * A.n;
+    CK(cudaMalloc(&A.ring, sizeof(double) * (size_t)std::max(1, A.nbnd) * 8 * A.nkmax * 10));
+    c->owned.push_back(A.ring);
+    CK(cudaMalloc(&A.flags, sizeof(unsigned) * 2 * (size_t)std::max(1, A.nbnd)));
+    c->owned.push_back(A.flags);
+    if (c->sa_pool) {  // the model's scalar sweeps run on the wide chunks too
+        CK(cudaMalloc(&A.sa, sizeof(double) * (6 * (size_t)A.n + 8)));
+        c->owned.push_back(A.sa);
+    }
+    W->chunks = c->up(W->hchunks);
+    c->wide = std::move(W);
+    L.wide = c->wide.get();
+    return 0;
+}
+
+static void wide_free(WcnsContext *c) {
+    if (!c->wide) return;
+    WideSweep &W = *c->wide;
+    free_owned(c, W.A.stat);
+    free_owned(c, W.A.ring);
+    free_owned(c, W.A.flags);
+    free_owned(c, W.A.sa);
+    free_owned(c, W.chunks);
+    c->wide.reset();
+    c->L.wide = nullptr;
+}
+
 // Line groups of the residual kernels for every direction (passes 2 and 3:
 // the mixed-precision kernels): at most inv_cap / vis_cap lines of a block
 // per CTA, fewer where the staged lines would pass 72 KB of shared memory.
@@ -551,28 +602,8 @@ static int build_tables(WcnsContext *c) {
         // cooperative sweeps, or, when those do not fit either, sweep plane by plane
         const bool want_plane = c->prm.flags & WCNS_FLAG_SWEEP_BY_PLANE, want_wide = c->prm.flags & WCNS_FLAG_SWEEP_WIDE;
         const bool clustered = !want_plane && !want_wide && setup_sweep(L, cl, fine) == 0;
-        if (!clustered && !want_plane) {
-            c->wide = std::make_unique<WideSweep>();
-            if (setup_sweep_wide(L, *c->wide) == 0) {
-                WideSweep &W = *c->wide;
-                WideArrays &A = W.A;
-                const size_t words = (size_t)(WIDE_COEF_WORDS + 5 + 5 + 15 + 5) * A.n + 8;
-                CK(cudaMalloc(&A.stat, sizeof(double) * words));
-                c->owned.push_back(A.stat);
-                A.rhs = A.stat + (size_t)WIDE_COEF_WORDS * A.n;
-                A.dql = A.rhs + (size_t)5 * A.n;
-                A.gs1 = A.dql + (size_t)5 * A.n;
-                A.gs2 = A.gs1 + (size_t)15 * A.n;
-                CK(cudaMalloc(&A.ring, sizeof(double) * (size_t)std::max(1, A.nbnd) * 8 * A.nkmax * 10));
-                c->owned.push_back(A.ring);
-                CK(cudaMalloc(&A.flags, sizeof(unsigned) * 2 * (size_t)std::max(1, A.nbnd)));
-                c->owned.push_back(A.flags);
-                W.chunks = c->up(W.hchunks);
-                L.wide = &W;
-            } else {
-                c->wide.reset();
-            }
-        }
+        if (!clustered && !want_plane)
+            if (int rc = wide_alloc(c); rc > 0) return rc;
         L.sweep_plane = !clustered && !L.wide ? 1 : 0;
     }
     // residual partials, update bad lists
@@ -1504,15 +1535,30 @@ extern "C" int wcns_get_shape(WcnsContext *c, int *shape) {
     return 0;
 }
 
+// a context whose blocks fit the clustered sweeps (its plane-major arrays
+// exist) can also sweep wide, and switch between the two
+static bool can_cluster(const WcnsContext *c) { return c->pm_pool != nullptr; }
+
 static int apply_shape(WcnsContext *c, const int *shape) {
     LaunchCtx &L = c->L;
-    if (clustered_sweeps(c) && (shape[0] != L.sweep_cluster || shape[1] != L.sweep_fine)) {
-        if (setup_sweep_exact(L, shape[0], shape[1])) {
-            set_err("wcns_set_shape: the blocks cannot be swept with " + std::to_string(shape[0]) +
-                    " CTAs per cluster in that lane mode");
-            return WCNS_ERR_ARGUMENT;
+    if (can_cluster(c) && !L.sweep_plane) {
+        if (shape[0] == 0) {  // wide sweeps
+            if (!L.wide) {
+                const int rc = wide_alloc(c);
+                if (rc) {
+                    if (rc < 0) set_err("wcns_set_shape: the blocks cannot be swept wide");
+                    return rc < 0 ? WCNS_ERR_ARGUMENT : rc;
+                }
+            }
+        } else if (L.wide || shape[0] != L.sweep_cluster || shape[1] != L.sweep_fine) {
+            if (setup_sweep_exact(L, shape[0], shape[1])) {
+                set_err("wcns_set_shape: the blocks cannot be swept with " + std::to_string(shape[0]) +
+                        " CTAs per cluster in that lane mode");
+                return WCNS_ERR_ARGUMENT;
+            }
+            c->PM.csize = L.sweep_cluster;
+            wide_free(c);
         }
-        c->PM.csize = L.sweep_cluster;
     }
     if (shape[2] != L.inv_cap || shape[3] != L.vis_cap)
         if (int rc = build_line_tables(c, shape[2], shape[3])) return rc;
@@ -1526,8 +1572,12 @@ extern "C" int wcns_set_shape(WcnsContext *c, const int *shape) {
         set_err("wcns_set_shape: lines per CTA must be in 1..32");
         return WCNS_ERR_ARGUMENT;
     }
-    if (clustered_sweeps(c) && (shape[0] < 1 || shape[1] < 0 || shape[1] > 1)) {
-        set_err("wcns_set_shape: the clustered sweeps need shape[0] >= 1 and shape[1] in 0..1");
+    if (shape[0] < 0 || shape[1] < 0 || shape[1] > 1) {
+        set_err("wcns_set_shape: shape[0] >= 0 (0: wide sweeps) and shape[1] in 0..1");
+        return WCNS_ERR_ARGUMENT;
+    }
+    if (!can_cluster(c) && shape[0] != 0) {
+        set_err("wcns_set_shape: these blocks only sweep wide or by plane (shape[0] = 0)");
         return WCNS_ERR_ARGUMENT;
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -1575,9 +1625,11 @@ extern "C" int wcns_autotune(WcnsContext *c, int reps, int *shape, double *ms) {
     int best[4];
     wcns_get_shape(c, best);
     double best_ms[3] = {0.0, 0.0, 0.0};
-    // the LU-SGS sweep shape
-    if (clustered_sweeps(c)) {
+    // the LU-SGS sweep form and shape: every cluster shape, and the wide sweeps
+    if (can_cluster(c) && !L.sweep_plane) {
         double tbest = 1e300;
+        const bool was_wide = L.wide != nullptr;
+        L.wide = nullptr;
         const int cls[5] = {1, 2, 4, 8, 16};
         for (int fine = 1; fine >= 0; fine--)
             for (int q = 0; q < 5; q++) {
@@ -1587,8 +1639,18 @@ extern "C" int wcns_autotune(WcnsContext *c, int reps, int *shape, double *ms) {
                 const double t = time_reps(c, reps, saved, [&] { launch_lhs(L); });
                 if (t < tbest) { tbest = t; best[0] = cand[0]; best[1] = cand[1]; }
             }
-        setup_sweep_exact(L, best[0], best[1]);
-        c->PM.csize = L.sweep_cluster;
+        if (was_wide) L.wide = c->wide.get();
+        const int wr = wide_alloc(c);
+        if (wr > 0) { cudaFree(saved); return wr; }
+        if (wr == 0) {
+            const double t = time_reps(c, reps, saved, [&] { launch_lhs(L); });
+            if (t < tbest) { tbest = t; best[0] = 0; best[1] = 0; }
+        }
+        if (best[0] > 0) {
+            setup_sweep_exact(L, best[0], best[1]);
+            c->PM.csize = L.sweep_cluster;
+            wide_free(c);
+        }
         best_ms[0] = tbest;
     }
     // lines per CTA of the residual kernels
