@@ -117,6 +117,11 @@ int wcns_get_interior(WcnsContext *ctx, int nfields, const int *fields, double *
 int wcns_boundary_all(WcnsContext *ctx);        /* exchange_bc + boundary_all (Main.f90:85-87) */
 int wcns_initial_q_dq_c_t(WcnsContext *ctx);    /* initial_q_dq_c_t (sub_tgh.f90:1-32) */
 int wcns_timestep(WcnsContext *ctx);            /* timestep_tgh (sub_tgh.f90:1270-1348) */
+/* wcns_rhs_vis without the SA model step: the node derivatives and the
+ * viscous flux only.  For a driver that advances the model itself
+ * (wcns_turbulence) between other work in the same step, e.g. a block-
+ * sharded run that refreshes its copies of other ranks' qke and vist. */
+int wcns_rhs_vis_flux(WcnsContext *ctx);
 int wcns_rhs_vis(WcnsContext *ctx);             /* r_h_s_vis (RHS.f90:2-30); with the SA model
                                                    set up it first runs the model step, see below */
 int wcns_communicate_dq(WcnsContext *ctx);      /* communicate_dq_npp (parallel.f90:3020-3058) */

@@ -1996,6 +1996,15 @@ int orc_rhs_vis(void *h) {
     return 0;
 }
 
+/* the viscous residual without the model step (a sharded run advances the
+ * model first and refreshes its proxies' qke and vist in between) */
+int orc_rhs_vis_flux(void *h) {
+    Orc *o = h;
+    if (o->prm.nvis != 1) return 0;
+    for (int nb = 1; nb <= o->nb; nb++) rhs_vis_block(o, &o->b[nb]);
+    return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* Interface averaging: communicate_dq_npp (parallel.f90:3020-3164) and */
 /* communicate_pv_npp (parallel.f90:3166-3326), one block per rank      */

@@ -44,6 +44,7 @@ int orc_boundary_all(void *h);
 int orc_initial_q_dq_c_t(void *h);
 int orc_timestep(void *h);
 int orc_rhs_vis(void *h);
+int orc_rhs_vis_flux(void *h);
 int orc_communicate_dq(void *h);
 int orc_rhs_invis(void *h);
 int orc_lhs(void *h);

@@ -26,15 +26,28 @@ class OracleBackend:
     def __init__(self, case):
         from oracle.pyoracle import Oracle
         self.o = Oracle(case)
+        self.sa = case.sa is not None
+        if self.sa:
+            self.o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"], distance=False)
 
     def phase(self, name):
         self.o.phase(name)
 
-    def get_state(self, nb):
-        return [self.o.get(n, nb) for n in shard.PRIM6]
+    def get_state(self, nb, fields=None):
+        names = fields or (shard.PRIM6 + (shard.SA2 if self.sa else ()))
+        return [self.o.get(n, nb) for n in names]
 
-    def set_state(self, nb, arrays):
-        self.o.set_prim(nb, arrays)
+    def set_state(self, nb, arrays, fields=None):
+        if fields is None:
+            self.o.set_prim(nb, arrays[:6])
+            for n, a in zip(shard.SA2 if self.sa else (), arrays[6:]):
+                self.o.set(n, nb, a)
+            return
+        for n, a in zip(fields, arrays):
+            self.o.set(n, nb, a)
+
+    def set_field(self, name, nb, arr):
+        self.o.set(name, nb, arr)
 
     def residual(self):
         res, rmax, _ = self.o.residual()
@@ -50,6 +63,19 @@ def laminar_channel():
     c.sa = None
     c.params.nvis = 1
     return c
+
+
+def sa_channel():
+    """The same 32 blocks with the Spalart-Allmaras model."""
+    return cases.channel_case(ni=97, nj=25, nk=17, bx=8, by=2, bz=2, first=1.0e-3)
+
+
+def full_distance(case):
+    """The whole case's wall distance per block (the oracle's exact minimum)."""
+    from oracle.pyoracle import Oracle
+    o = Oracle(case)
+    o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
+    return {g: o.get("dist", g) for g in range(1, case.nblocks + 1)}
 
 
 def slabs(case, nranks):
@@ -87,13 +113,18 @@ def test_rank_case_records_point_back():
             full = int(np.sum(c.regions[:, 0] == g))
             if owned[i]:
                 assert len(per[i + 1]) == full
+    # a proxy thinner than 7 points that loses regions next to an owned block
+    thin = cases.channel_case(ni=33, nj=25, nk=17, bx=8, by=2, bz=2, first=1.0e-3)
+    thin.sa = None
     with pytest.raises(ValueError):
-        shard.rank_case(cases.small_channel_case(), [0] * 24, 0)
+        shard.rank_case(thin, slabs(thin, 2), 0, hops=1)
 
 
 def _single(case, n):
     from oracle.pyoracle import Oracle
     o = Oracle(case)
+    if case.sa:
+        o.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
     h = o.step(n)
     return o, h
 
@@ -105,18 +136,19 @@ def _compare(case, ranks, ref, owners):
             if owners[g - 1] != rk.rank:
                 continue
             d = case.dims[g - 1]
-            for n in ("r", "u", "v", "w", "p"):
+            for n in ("r", "u", "v", "w", "p") + (("qke", "vist") if case.sa else ()):
                 a, b = interior(rk.get(n, g), d), interior(ref.get(n, g), d)
                 worst = max(worst, float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), 0.3))
     return worst
 
 
-@pytest.mark.parametrize("which", ["plate_lpt", "channel_slabs"])
+@pytest.mark.parametrize("which", ["plate_lpt", "channel_slabs", "sa_channel_slabs"])
 def test_sharded_oracle_in_one_process_matches_single(which):
-    case = cases.small_plate_case() if which == "plate_lpt" else laminar_channel()
+    case = {"plate_lpt": cases.small_plate_case, "channel_slabs": laminar_channel, "sa_channel_slabs": sa_channel}[which]()
     owners = shard.lpt_partition(case.dims, 2) if which == "plate_lpt" else slabs(case, 2)
     n = 4
-    ranks, hist = shard.run_local(case, 2, n, OracleBackend, owners=owners)
+    dist = full_distance(case) if case.sa else None
+    ranks, hist = shard.run_local(case, 2, n, OracleBackend, owners=owners, dist=dist)
     ref, href = _single(case, n)
     worst = _compare(case, ranks, ref, owners)
     print(f"{which}: owned blocks vs single oracle, max rel {worst:.2e}; rms {hist[-1]:.6e} vs {href[-1]:.6e}")
@@ -175,14 +207,18 @@ def test_gloo_two_ranks_exchange_matches_single():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("which", ["plate_lpt", "channel_slabs"])
+@pytest.mark.parametrize("which", ["plate_lpt", "channel_slabs", "sa_channel_slabs"])
 def test_sharded_gpu_contexts_match_one_context(which):
     from wcns_b200.solver import Wcns
-    case = cases.small_plate_case() if which == "plate_lpt" else laminar_channel()
+    case = {"plate_lpt": cases.small_plate_case, "channel_slabs": laminar_channel, "sa_channel_slabs": sa_channel}[which]()
     owners = shard.lpt_partition(case.dims, 2) if which == "plate_lpt" else slabs(case, 2)
     n = 4
-    ranks, hist = shard.run_local(case, 2, n, shard.GpuBackend, owners=owners)
     ref = Wcns(case)
+    dist = None
+    if case.sa:
+        ref.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
+        dist = {g: ref.get("dist", g) for g in range(1, case.nblocks + 1)}
+    ranks, hist = shard.run_local(case, 2, n, shard.GpuBackend, owners=owners, dist=dist)
     href = ref.step(n)
     worst = _compare(case, ranks, ref, owners)
     print(f"{which} on the GPU: owned blocks vs one context, max rel {worst:.2e}")

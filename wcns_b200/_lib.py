@@ -52,6 +52,7 @@ SIGNATURES = {
     "wcns_sweep_mode": (C.c_int, [_VP]),
     "wcns_set_precision": (C.c_int, [_VP, C.c_int]),
     "wcns_get_precision": (C.c_int, [_VP]),
+    "wcns_rhs_vis_flux": (C.c_int, [_VP]),
     "wcns_get_shape": (C.c_int, [_VP, _VP]),
     "wcns_device_name": (C.c_int, [_VP, C.c_char_p, C.c_int]),
     "wcns_set_shape": (C.c_int, [_VP, _VP]),

@@ -1247,6 +1247,12 @@ PHASE(wcns_rhs_vis, if (c->P.nvis == 1) {
     launch_node_derivatives(c->L);
     launch_rhs_dirs(c->L, true);
 })
+// the viscous residual without the model step (a driver that advances the
+// SA model itself with wcns_turbulence, e.g. a sharded run)
+PHASE(wcns_rhs_vis_flux, if (c->P.nvis == 1) {
+    launch_node_derivatives(c->L);
+    launch_rhs_dirs(c->L, true);
+})
 PHASE(wcns_communicate_dq, launch_communicate(c->L, 0))
 PHASE(wcns_turbulence, {
     if (!c->sa_pool) { set_err("wcns_turbulence: wcns_sa_setup was not called"); return WCNS_ERR_ARGUMENT; }

@@ -26,8 +26,11 @@ owned block, since E1 and E3 overwrite them first; the one local dependence
 reading the proxy's ghosts towards an absent block -- needs the two faces
 to be at least seven points apart, which `rank_case` checks.
 
-The Spalart-Allmaras model is not sharded: its scalar sweep inside the
-viscous phase would need one more exchange.  The exchange moves whole
+With the Spalart-Allmaras model the state also carries qke and vist, the
+model step runs as its own phase, and a third exchange (E2) refreshes the
+proxies' qke and vist after it, before the viscous flux; the wall distance
+of every block is the whole case's (`set_distance`), not the distance to
+the walls a rank happens to hold.  The exchange moves whole
 blocks through host arrays (a transport: `DistTransport` over
 torch.distributed, `LocalTransport` between contexts of one process); a
 production form would pack the three-layer halos and interface faces on
@@ -42,6 +45,7 @@ import numpy as np
 from .cases import Case, Params
 
 PRIM6 = ("r", "u", "v", "w", "p", "t")
+SA2 = ("qke", "vist")
 
 
 def lpt_partition(dims, nranks):
@@ -84,8 +88,6 @@ def rank_case(case: Case, owners, rank, hops=3):
     partner is absent is dropped (a proxy's ghosts there keep the owner's
     values), and the partner-region indices (ibcwin) are renumbered.
     Returns (case, local->global block numbers, owned mask)."""
-    if case.sa:
-        raise ValueError("block sharding covers laminar and Euler cases (the SA sweep needs another exchange)")
     owned, local = local_blocks(case, owners, rank, hops)
     gmap = {g: i + 1 for i, g in enumerate(local)}
     regs_of = {b: [r for r in case.regions if int(r[0]) == b] for b in local}
@@ -116,7 +118,7 @@ def rank_case(case: Case, owners, rank, hops=3):
     prm = Params(**{k: getattr(case.params, k) for k in Params.__dataclass_fields__})
     sub = Case(f"{case.name}_rank{rank}", prm, [case.dims[b - 1] for b in local], [case.xyz[b - 1] for b in local],
                np.array(rows, dtype=np.int32), [case.prim[b - 1] for b in local], case.nsteps,
-               f"rank {rank}: owned {owned}, proxies {[b for b in local if b not in owned]}")
+               f"rank {rank}: owned {owned}, proxies {[b for b in local if b not in owned]}", sa=case.sa)
     return sub, local, [b in owned for b in local]
 
 
@@ -162,17 +164,35 @@ class GpuBackend:
     def __init__(self, case, flags=0):
         from .solver import Wcns
         self.g = Wcns(case, flags=flags)
+        self.sa = case.sa is not None
+        if self.sa:
+            self.g.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
 
     def phase(self, name):
         getattr(self.g, {"boundary_all": "boundary_all", "initial_q_dq_c_t": "initial_q_dq_c_t",
-                         "timestep": "timestep_tgh", "rhs_vis": "r_h_s_vis", "communicate_dq": "communicate_dq_npp",
+                         "timestep": "timestep_tgh", "rhs_vis": "r_h_s_vis", "rhs_vis_flux": "r_h_s_vis_flux",
+                         "turbulence": "turbulence", "communicate_dq": "communicate_dq_npp",
                          "rhs_invis": "r_h_s_invis", "lhs": "l_h_s_tgh", "communicate_pv": "communicate_pv_npp"}[name])()
 
-    def get_state(self, nb):
-        return self.g.get_prim(nb)
+    def get_state(self, nb, fields=None):
+        """The ghosted arrays of `fields` (default: r,u,v,w,p,T and, with the
+        SA model, qke and vist)."""
+        if fields is None:
+            out = list(self.g.get_prim(nb))
+            return out + [self.g.get(n, nb) for n in SA2] if self.sa else out
+        return [self.g.get(n, nb) for n in fields]
 
-    def set_state(self, nb, arrays):
-        self.g.set_prim(nb, arrays)
+    def set_state(self, nb, arrays, fields=None):
+        if fields is None:
+            self.g.set_prim(nb, arrays[:6])
+            for n, a in zip(SA2 if self.sa else (), arrays[6:]):
+                self.g.set(n, nb, a)
+            return
+        for n, a in zip(fields, arrays):
+            self.g.set(n, nb, a)
+
+    def set_field(self, name, nb, arr):
+        self.g.set(name, nb, arr)
 
     def residual(self):
         res, rmax, _ = self.g.residual_curve()
@@ -191,39 +211,62 @@ class ShardedRank:
         self.lmap = {g: i + 1 for i, g in enumerate(self.local)}
         self.be = backend(self.sub) if callable(backend) else backend
         self.tr = transport
+        self.sa = case.sa is not None
         # every block held as a proxy somewhere: the exchanges walk these in
         # global order on every rank (the same collective sequence everywhere)
         self.shared = sorted({b for r in range(max(self.owners) + 1)
                               for b in local_blocks(case, self.owners, r)[1] if self.owners[b - 1] != r})
 
-    def _exchange(self):
+    def fields(self, which):
+        """The exchanged arrays: the whole state (E1, E3) or qke and vist (E2)."""
+        if which == "sa":
+            return SA2
+        return PRIM6 + (SA2 if self.sa else ())
+
+    def set_distance(self, dist):
+        """The wall distance of every local block from {global block: ghosted
+        array} of the whole case (after the backend's SA set-up)."""
+        for g, nb in self.lmap.items():
+            self.be.set_field("dist", nb, dist[g])
+
+    def _exchange(self, which="state"):
         """One exchange over a DistTransport: every shared block broadcast
         from its owner, in global block order on every rank."""
+        names = self.fields(which)
         for b in self.shared:
             owner = self.owners[b - 1]
             ni, nj, nk = self.case.dims[b - 1]
-            arrays = self.be.get_state(self.lmap[b]) if self.rank == owner else [(nk + 6, nj + 6, ni + 6)] * 6
+            arrays = (self.be.get_state(self.lmap[b], names) if self.rank == owner
+                      else [(nk + 6, nj + 6, ni + 6)] * len(names))
             got = self.tr.share(b, owner, self.rank, arrays)
             if self.rank != owner and b in self.lmap:
-                self.be.set_state(self.lmap[b], got)
+                self.be.set_state(self.lmap[b], got, names)
 
-    def publish(self, store):
-        """LocalTransport: the states of the owned blocks others hold."""
+    def publish(self, store, which="state"):
+        """LocalTransport: the arrays of the owned blocks others hold."""
+        names = self.fields(which)
         for b in self.shared:
             if self.owners[b - 1] == self.rank:
-                store[b] = [a.copy() for a in self.be.get_state(self.lmap[b])]
+                store[b] = [a.copy() for a in self.be.get_state(self.lmap[b], names)]
 
-    def pull(self, store):
-        """LocalTransport: every proxy's state from the store."""
+    def pull(self, store, which="state"):
+        """LocalTransport: every proxy's arrays from the store."""
+        names = self.fields(which)
         for b in self.shared:
             if self.owners[b - 1] != self.rank and b in self.lmap:
-                self.be.set_state(self.lmap[b], store[b])
+                self.be.set_state(self.lmap[b], store[b], names)
 
-    def phases_to_update(self):
+    def phases_to_model(self):
+        """From the BCs to the SA model step (E1 before it)."""
         for name in ("boundary_all", "initial_q_dq_c_t", "timestep"):
             self.be.phase(name)
+        if self.sa:
+            self.be.phase("turbulence")
+
+    def phases_to_update(self):
+        """From the viscous flux to the update (E2 before it with the SA model)."""
         if self.case.params.nvis == 1:
-            self.be.phase("rhs_vis")
+            self.be.phase("rhs_vis_flux" if self.sa else "rhs_vis")
             self.be.phase("communicate_dq")
         self.be.phase("rhs_invis")
         self.be.phase("communicate_dq")
@@ -242,12 +285,16 @@ class ShardedRank:
 
     def step(self, nsteps=1):
         """nsteps whole steps over a DistTransport (every rank calls it):
-        E1, the phases up to the update, E3, the prim averaging; the
-        residual RMS of every step from an all-reduce of the block sums."""
+        E1, the phases to the model step, E2 (SA), the phases to the update,
+        E3, the prim averaging; the residual RMS of every step from an
+        all-reduce of the block sums."""
         import torch
         hist = []
         for _ in range(nsteps):
             self._exchange()  # E1
+            self.phases_to_model()
+            if self.sa:
+                self._exchange("sa")  # E2
             self.phases_to_update()
             self._exchange()  # E3
             mine = self.finish_after_e3()
@@ -272,27 +319,39 @@ def rms_of(block_res):
     return float(np.sqrt(total / npts))
 
 
-def run_local(case, nranks, nsteps, backend, owners=None):
+def run_local(case, nranks, nsteps, backend, owners=None, dist=None):
     """All ranks in one process, in turn: each step every rank publishes its
-    owned states, pulls its proxies (E1) and runs up to the update; then
-    every rank publishes its updated states, pulls (E3), averages prim and
-    reports its residual means.  Returns the ranks and the residual RMS of
-    every step."""
+    owned states, pulls its proxies (E1) and runs to the model step; with
+    the SA model the ranks then exchange qke and vist (E2); every rank runs
+    to the update, publishes its updated states, pulls (E3), averages prim
+    and reports its residual means.  `dist` ({global block: ghosted array})
+    sets the whole case's wall distance.  Returns the ranks and the
+    residual RMS of every step."""
     owners = list(owners) if owners is not None else lpt_partition(case.dims, nranks)
     tr = LocalTransport()
     ranks = [ShardedRank(case, owners, r, backend, tr) for r in range(nranks)]
+    if dist is not None:
+        for rk in ranks:
+            rk.set_distance(dist)
+
+    def exchange(which):
+        for rk in ranks:
+            rk.publish(tr.store, which)
+        for rk in ranks:
+            rk.pull(tr.store, which)
+
     hist = []
     for _ in range(nsteps):
+        exchange("state")
         for rk in ranks:
-            rk.publish(tr.store)
+            rk.phases_to_model()
+        if case.sa is not None:
+            exchange("sa")
         for rk in ranks:
-            rk.pull(tr.store)
             rk.phases_to_update()
-        for rk in ranks:
-            rk.publish(tr.store)
+        exchange("state")
         res = {}
         for rk in ranks:
-            rk.pull(tr.store)
             res.update(rk.finish_after_e3())
         hist.append(rms_of(res))
     return ranks, np.array(hist)

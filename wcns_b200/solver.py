@@ -230,6 +230,10 @@ class Wcns:
     def r_h_s_vis(self):
         _check(_lib.load().wcns_rhs_vis(self.h))
 
+    def r_h_s_vis_flux(self):
+        """r_h_s_vis without the SA model step (wcns_rhs_vis_flux)."""
+        _check(_lib.load().wcns_rhs_vis_flux(self.h))
+
     def communicate_dq_npp(self):
         _check(_lib.load().wcns_communicate_dq(self.h))
 
