@@ -84,6 +84,12 @@ const char *wcns_last_error(void);
 int wcns_set_prim(WcnsContext *ctx, int nb, const double *r, const double *u, const double *v, const double *w,
                   const double *p, const double *t);
 int wcns_get_field(WcnsContext *ctx, int field, int nb, double *out);
+/* The device address of block nb's slice of a field (the ghosted layout of
+ * wcns_get_field) and its number of doubles, for exchanges that stay on the
+ * device (peer copies, NCCL).  Work on the context's stream must be finished
+ * (wcns_sync) before the slice is read or written another way, and that
+ * access finished before the context's next call. */
+int wcns_field_device_ptr(WcnsContext *ctx, int field, int nb, void **ptr, long long *count);
 /* The primitive state of block nb (r, u, v, w, p, t; t may be NULL) in the
  * ghosted layout of wcns_set_prim, with one synchronisation for the block:
  * what the flow-file write reads per block (write_flow_file_parallel,

@@ -56,3 +56,22 @@ def test_set_interior_writes_interior_only_and_skips_null_blocks():
     five = g.get_interior(["r", "u", "v", "w", "p"])
     for nb in range(1, case.nblocks + 1):
         np.testing.assert_array_equal(five[nb - 1][4], interior(g.get("p", nb), case.dims[nb - 1]))
+
+
+def test_device_view_aliases_the_field():
+    """wcns_field_device_ptr: a CUDA tensor over a block's field slice reads
+    the field and writes into it (after the context's stream is idle)."""
+    import torch
+    from wcns_b200.solver import Wcns
+    case = cases.small_plate_case()
+    g = Wcns(case)
+    g.step(1, history=False)
+    g.sync()
+    t = torch.as_tensor(g.device_view("p", 2), device="cuda")
+    orig = g.get("p", 2)
+    np.testing.assert_array_equal(t.cpu().numpy(), orig)
+    before = g.get("r", 2)
+    t.mul_(2.0)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(g.get("p", 2), 2.0 * orig)
+    np.testing.assert_array_equal(g.get("r", 2), before)

@@ -207,8 +207,9 @@ def test_gloo_two_ranks_exchange_matches_single():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("device", [False, True])
 @pytest.mark.parametrize("which", ["plate_lpt", "channel_slabs", "sa_channel_slabs"])
-def test_sharded_gpu_contexts_match_one_context(which):
+def test_sharded_gpu_contexts_match_one_context(which, device):
     from wcns_b200.solver import Wcns
     case = {"plate_lpt": cases.small_plate_case, "channel_slabs": laminar_channel, "sa_channel_slabs": sa_channel}[which]()
     owners = shard.lpt_partition(case.dims, 2) if which == "plate_lpt" else slabs(case, 2)
@@ -218,9 +219,9 @@ def test_sharded_gpu_contexts_match_one_context(which):
     if case.sa:
         ref.sa_setup(case.sa["timedt_turb"], case.sa["kmaxlim"])
         dist = {g: ref.get("dist", g) for g in range(1, case.nblocks + 1)}
-    ranks, hist = shard.run_local(case, 2, n, shard.GpuBackend, owners=owners, dist=dist)
+    ranks, hist = shard.run_local(case, 2, n, shard.GpuBackend, owners=owners, dist=dist, device=device)
     href = ref.step(n)
     worst = _compare(case, ranks, ref, owners)
-    print(f"{which} on the GPU: owned blocks vs one context, max rel {worst:.2e}")
+    print(f"{which} on the GPU ({'device' if device else 'host'} exchange): owned blocks vs one context, max rel {worst:.2e}")
     assert worst <= 1e-13
     np.testing.assert_allclose(hist, href, rtol=1e-12)

@@ -53,6 +53,7 @@ SIGNATURES = {
     "wcns_set_precision": (C.c_int, [_VP, C.c_int]),
     "wcns_get_precision": (C.c_int, [_VP]),
     "wcns_rhs_vis_flux": (C.c_int, [_VP]),
+    "wcns_field_device_ptr": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
     "wcns_get_shape": (C.c_int, [_VP, _VP]),
     "wcns_device_name": (C.c_int, [_VP, C.c_char_p, C.c_int]),
     "wcns_set_shape": (C.c_int, [_VP, _VP]),

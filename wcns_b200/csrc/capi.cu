@@ -926,6 +926,19 @@ extern "C" int wcns_get_field(WcnsContext *c, int field, int nb, double *out) {
     return 0;
 }
 
+// Device address of block nb's ghosted slice of a public field and its
+// element count; the caller synchronises with the context's stream
+// (wcns_sync) before reading or writing through it.
+extern "C" int wcns_field_device_ptr(WcnsContext *c, int field, int nb, void **ptr, long long *count) {
+    const DevBlock *d;
+    if (int rc = block_range(c, nb, &d)) return rc;
+    double *base = field_base(c, field);
+    if (!base || !ptr || !count) { set_err("wcns_field_device_ptr: unsupported field or null output"); return WCNS_ERR_UNSUPPORTED; }
+    *ptr = base + d->off;
+    *count = (long long)d->gx * d->gy * d->gz;
+    return 0;
+}
+
 extern "C" int wcns_get_prim(WcnsContext *c, int nb, double *r, double *u, double *v, double *w, double *p, double *t) {
     const DevBlock *d;
     if (int rc = block_range(c, nb, &d)) return rc;

@@ -31,10 +31,13 @@ model step runs as its own phase, and a third exchange (E2) refreshes the
 proxies' qke and vist after it, before the viscous flux; the wall distance
 of every block is the whole case's (`set_distance`), not the distance to
 the walls a rank happens to hold.  The exchange moves whole
-blocks through host arrays (a transport: `DistTransport` over
-torch.distributed, `LocalTransport` between contexts of one process); a
-production form would pack the three-layer halos and interface faces on
-the device and send them with NCCL.
+blocks, either through host arrays (`DistTransport` over torch.distributed,
+`LocalTransport` between contexts of one process) or on the device: the
+contexts' field slices are wrapped as CUDA tensors (wcns_field_device_ptr)
+and broadcast in place over NCCL (`DeviceTransport`), or copied device to
+device between the contexts of one process (`run_local(..., device=True)`).
+Packing only the three-layer halos and interface faces would cut the bytes
+further.
 """
 from __future__ import annotations
 
@@ -156,6 +159,24 @@ class DistTransport:
         return out
 
 
+class DeviceTransport:
+    """torch.distributed over NCCL on the contexts' own device memory: each
+    array of a shared block is broadcast from its owner's field slice
+    straight into the proxies' slices (a rank that does not hold the block
+    receives into scratch)."""
+
+    device = True
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist, self.group = dist, group
+
+    def share(self, block, owner, rank, tensors):
+        for t in tensors:
+            self.dist.broadcast(t, src=owner, group=self.group)
+        return tensors
+
+
 # --------------------------------------------------------------------------
 # a backend runs the reference's phases on a rank's case: GpuBackend here
 # (the tests add one over the CPU oracle, which is their checker)
@@ -194,6 +215,14 @@ class GpuBackend:
     def set_field(self, name, nb, arr):
         self.g.set(name, nb, arr)
 
+    def device_views(self, nb, fields):
+        """CUDA tensors aliasing block nb's slices of `fields`."""
+        import torch
+        return [torch.as_tensor(self.g.device_view(n, nb), device="cuda") for n in fields]
+
+    def sync(self):
+        self.g.sync()
+
     def residual(self):
         res, rmax, _ = self.g.residual_curve()
         return res, rmax
@@ -230,9 +259,21 @@ class ShardedRank:
             self.be.set_field("dist", nb, dist[g])
 
     def _exchange(self, which="state"):
-        """One exchange over a DistTransport: every shared block broadcast
-        from its owner, in global block order on every rank."""
+        """One exchange over a DistTransport or a DeviceTransport: every
+        shared block broadcast from its owner, in global block order on
+        every rank."""
         names = self.fields(which)
+        if getattr(self.tr, "device", False):
+            import torch
+            self.be.sync()
+            torch.cuda.synchronize()
+            for b in self.shared:
+                ni, nj, nk = self.case.dims[b - 1]
+                ts = (self.be.device_views(self.lmap[b], names) if b in self.lmap else
+                      [torch.empty((nk + 6, nj + 6, ni + 6), dtype=torch.float64, device="cuda") for _ in names])
+                self.tr.share(b, self.owners[b - 1], self.rank, ts)
+            torch.cuda.synchronize()
+            return
         for b in self.shared:
             owner = self.owners[b - 1]
             ni, nj, nk = self.case.dims[b - 1]
@@ -319,7 +360,7 @@ def rms_of(block_res):
     return float(np.sqrt(total / npts))
 
 
-def run_local(case, nranks, nsteps, backend, owners=None, dist=None):
+def run_local(case, nranks, nsteps, backend, owners=None, dist=None, device=False):
     """All ranks in one process, in turn: each step every rank publishes its
     owned states, pulls its proxies (E1) and runs to the model step; with
     the SA model the ranks then exchange qke and vist (E2); every rank runs
@@ -335,6 +376,21 @@ def run_local(case, nranks, nsteps, backend, owners=None, dist=None):
             rk.set_distance(dist)
 
     def exchange(which):
+        if device:  # device-to-device copies from the owners' slices into the proxies'
+            import torch
+            for rk in ranks:
+                rk.be.sync()
+            torch.cuda.synchronize()
+            names = ranks[0].fields(which)
+            for rk in ranks:
+                for b in rk.shared:
+                    own = ranks[owners[b - 1]]
+                    if own is rk or b not in rk.lmap:
+                        continue
+                    for dst, src in zip(rk.be.device_views(rk.lmap[b], names), own.be.device_views(own.lmap[b], names)):
+                        dst.copy_(src)
+            torch.cuda.synchronize()
+            return
         for rk in ranks:
             rk.publish(tr.store, which)
         for rk in ranks:

@@ -22,6 +22,14 @@ FID = {n: i for i, n in enumerate(FIELDS)}
 FORCE_KEYS = ("cfx", "cfy", "cfz", "cmx", "cmy", "cmz", "cl", "cd", "xcp")
 
 
+class _DeviceSlice:
+    """A device array described by __cuda_array_interface__ (version 3)."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 3, "strides": None, "stream": None}
+
+
 class WcnsError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"[{code}] {msg}")
@@ -212,6 +220,18 @@ class Wcns:
         n = C.c_int(0)
         _check(_lib.load().wcns_profile_step(self.h, cap, ms.ctypes.data, names, C.byref(n)))
         return [(names[q].decode(), float(ms[q])) for q in range(n.value)]
+
+    def device_view(self, name, nb):
+        """Block nb's ghosted slice of a field on the device, as an object
+        with __cuda_array_interface__ (shape (nk+6, nj+6, ni+6), float64):
+        torch.as_tensor(view, device="cuda") aliases the context's memory.
+        Call sync() before touching it and synchronise after."""
+        ptr, count = C.c_void_p(), C.c_longlong()
+        _check(_lib.load().wcns_field_device_ptr(self.h, FID[name], nb, C.byref(ptr), C.byref(count)))
+        ni, nj, nk = self.dims[nb - 1]
+        if count.value != (nk + 6) * (nj + 6) * (ni + 6):
+            raise RuntimeError("unexpected field slice size")
+        return _DeviceSlice(int(ptr.value), (nk + 6, nj + 6, ni + 6))
 
     def set(self, name, nb, arr):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
