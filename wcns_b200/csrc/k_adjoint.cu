@@ -278,10 +278,11 @@ __device__ __forceinline__ void flux_t(const DevParams &P, const T *ql, const T 
 // accumulators), the line's lambda 5 x n, the metrics 3 x n, the half-node
 // tangent fluxes 5 x (n+1); odd, so that the lines of a group fall on
 // different banks
-__host__ __device__ inline int adj_line_stride(int n) { return (10 * (n + 6) + 8 * n + 5 * (n + 1)) | 1; }
+__host__ __device__ inline int adj_line_stride(int n) { return (10 * (n + 6) + 8 * n + 15 * (n + 1)) | 1; }
 
 struct AdjLine {
     double *q, *x, *lam, *sk, *fd;  // x: tangent (jvp) or accumulated adjoint (vjp)
+    double *sb;  // (vjp) adjoint of the WCNS left (m*(n+1)+h) and right ((5+m)*(n+1)+h) states
     long long stride, base;          // base: field index of position l = 0
     int n, ist, ied;
 };
@@ -303,6 +304,7 @@ __device__ __forceinline__ void adj_line_init(AdjLine &L, double *smem, int ln, 
     L.lam = S + 10 * W;
     L.sk = L.lam + 5 * n;
     L.fd = L.sk + 3 * n;
+    L.sb = L.fd + 5 * (n + 1);
     L.ist = F.f[F_R][L.base - 2 * L.stride] < SMALL ? 2 : 0;
     L.ied = F.f[F_R][L.base + (long long)(n + 3) * L.stride] < SMALL ? n - 2 : n;
 }
@@ -397,29 +399,22 @@ __device__ __forceinline__ double dxyz_coef(int n, int l, int h) {
     return flux_dxyz_at(ind, n, l);
 }
 
-// adds the adjoint `sbar` of one half-node state of variable m to the line's
-// point adjoints: through the closure, or through WCNS-E-5 with the weights
-// recomputed (their derivatives from five dual tangents)
-__device__ __forceinline__ void state_adjoint(const AdjLine &L, bool left, int h, int m, double sbar) {
-    if (sbar == 0.0) return;
+// routes the adjoint `sbar` of one half-node state of variable m: through
+// the closure's constant coefficients into the line's point adjoints, or
+// into the line's state adjoints for the WCNS phase; returns nothing to do
+// when it is zero
+__device__ __forceinline__ void route_state(const AdjLine &L, bool left, int h, int m, double sbar) {
     double c[4];
     int l[4];
+    const int H = L.n + 1;
+    double &slot = L.sb[(left ? m : 5 + m) * H + h];
     if (closure(L.n, L.ist, L.ied, left, h, c, l)) {
-        for (int j = 0; j < 4; j++) atomicAdd(&aq(L, L.x, m, l[j]), c[j] * sbar);
+        slot = 0.0;
+        if (sbar != 0.0)
+            for (int j = 0; j < 4; j++) atomicAdd(&aq(L, L.x, m, l[j]), c[j] * sbar);
         return;
     }
-    const int i = left ? h : h + 1;
-    Dual<5> s[5];
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-        s[k] = dconst<5>(aq(L, L.q, m, i - 2 + k));
-        s[k].d[k] = 1.0;
-    }
-    Dual<5> ql, qr;
-    wcns_states<Dual<5>>(s[0], s[1], s[2], s[3], s[4], ql, qr);
-    const Dual<5> &st = left ? ql : qr;
-#pragma unroll
-    for (int k = 0; k < 5; k++) atomicAdd(&aq(L, L.x, m, i - 2 + k), st.d[k] * sbar);
+    slot = sbar;
 }
 }  // namespace
 
@@ -465,12 +460,11 @@ __global__ void __launch_bounds__(256) k_rhs_invis_vjp(DevParams P, DevFields F,
 #pragma unroll
                 for (int m = 0; m < 5; m++) fb[m] += cf * L.lam[m * n + l - 1];
         }
-        // the states as the residual forms them, then the flux's Jacobian
-        // over the ten state components (left 0..4, right 5..9)
-        Dual<10> ql[5], qr[5], f[5];
+        // the states as the residual forms them, then the flux's Jacobian,
+        // one side's five components at a time (left, then right)
+        double vl[5], vr[5];
         bool fall_l, fall_r;
         {
-            double vl[5], vr[5];
 #pragma unroll
             for (int m = 0; m < 5; m++) {
                 auto get = [&](int l) { return aq(L, L.q, m, l); };
@@ -482,36 +476,73 @@ __global__ void __launch_bounds__(256) k_rhs_invis_vjp(DevParams P, DevFields F,
             const int il = h > 1 ? h : 1, ir = h + 1 < n ? h + 1 : n;
 #pragma unroll
             for (int m = 0; m < 5; m++) {
-                ql[m] = dconst<10>(fall_l ? aq(L, L.q, m, il) : vl[m]);
-                qr[m] = dconst<10>(fall_r ? aq(L, L.q, m, ir) : vr[m]);
-                ql[m].d[m] = 1.0;
-                qr[m].d[5 + m] = 1.0;
+                if (fall_l) vl[m] = aq(L, L.q, m, il);
+                if (fall_r) vr[m] = aq(L, L.q, m, ir);
             }
         }
         auto ax = [&](int l) { return L.sk[l - 1]; };
         auto ay = [&](int l) { return L.sk[n + l - 1]; };
         auto az = [&](int l) { return L.sk[2 * n + l - 1]; };
-        flux_t(P, ql, qr, value_half_node_at(ax, n, h), value_half_node_at(ay, n, h), value_half_node_at(az, n, h), f);
+        const double kx = value_half_node_at(ax, n, h), ky = value_half_node_at(ay, n, h), kz = value_half_node_at(az, n, h);
         double qlb[5], qrb[5];
-#pragma unroll
-        for (int j = 0; j < 5; j++) {
-            double a = 0.0, b = 0.0;
+#pragma unroll 1
+        for (int side = 0; side < 2; side++) {
+            Dual<5> ql[5], qr[5], f[5];
 #pragma unroll
             for (int m = 0; m < 5; m++) {
-                a += fb[m] * f[m].d[j];
-                b += fb[m] * f[m].d[5 + j];
+                ql[m] = dconst<5>(vl[m]);
+                qr[m] = dconst<5>(vr[m]);
+                if (side == 0) ql[m].d[m] = 1.0;
+                else qr[m].d[m] = 1.0;
             }
-            qlb[j] = a;
-            qrb[j] = b;
+            flux_t(P, ql, qr, kx, ky, kz, f);
+            double *dst = side == 0 ? qlb : qrb;
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                double a = 0.0;
+#pragma unroll
+                for (int m = 0; m < 5; m++) a += fb[m] * f[m].d[j];
+                dst[j] = a;
+            }
         }
         const int il = h > 1 ? h : 1, ir = h + 1 < n ? h + 1 : n;
 #pragma unroll
         for (int m = 0; m < 5; m++) {
-            if (fall_l) atomicAdd(&aq(L, L.x, m, il), qlb[m]);
-            else state_adjoint(L, true, h, m, qlb[m]);
-            if (fall_r) atomicAdd(&aq(L, L.x, m, ir), qrb[m]);
-            else state_adjoint(L, false, h, m, qrb[m]);
+            if (fall_l) {
+                atomicAdd(&aq(L, L.x, m, il), qlb[m]);
+                L.sb[m * H + h] = 0.0;
+            } else {
+                route_state(L, true, h, m, qlb[m]);
+            }
+            if (fall_r) {
+                atomicAdd(&aq(L, L.x, m, ir), qrb[m]);
+                L.sb[(5 + m) * H + h] = 0.0;
+            } else {
+                route_state(L, false, h, m, qrb[m]);
+            }
         }
+    }
+    __syncthreads();
+    // WCNS-E-5 transposed, per (line, variable, point i): the left state at
+    // half node i and the right state at half node i-1 come from the same
+    // stencil q(i-2..i+2); one evaluation with five dual tangents recomputes
+    // the weights and gives both states' derivatives
+    for (int e = threadIdx.x; e < NL * 5 * (n + 2); e += blockDim.x) {
+        const int ln = e / (5 * (n + 2)), r = e - ln * 5 * (n + 2), m = r / (n + 2), i = r - m * (n + 2);
+        const AdjLine &L = lines[ln];
+        const double a = i <= n ? L.sb[m * H + i] : 0.0;
+        const double b = i >= 1 ? L.sb[(5 + m) * H + i - 1] : 0.0;
+        if (a == 0.0 && b == 0.0) continue;
+        Dual<5> sv[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            sv[k] = dconst<5>(aq(L, L.q, m, i - 2 + k));
+            sv[k].d[k] = 1.0;
+        }
+        Dual<5> ql, qr;
+        wcns_states<Dual<5>>(sv[0], sv[1], sv[2], sv[3], sv[4], ql, qr);
+#pragma unroll
+        for (int k = 0; k < 5; k++) atomicAdd(&aq(L, L.x, m, i - 2 + k), ql.d[k] * a + qr.d[k] * b);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < NL * W * 5; e += blockDim.x) {
