@@ -213,3 +213,23 @@ def test_force_of_uniform_pressure_on_flat_wall(oracle_lib):
     assert abs(f["cfx"]) < 1e-15 and abs(f["cfz"]) < 1e-15
     assert f["cmx"] == pytest.approx(2 * dp * mx, rel=1e-12)
     assert f["cmz"] == pytest.approx(-2 * dp * mz, rel=1e-12)
+
+
+def test_flux_dxyz_interior_telescopes(L):
+    """Discrete conservation of the interior difference: over the points
+    3..n-2 the 6th-order FLUX_DXYZ is the difference of a numerical flux,
+    G(l) = 2250 f(l) - 125 (f(l-1)+f(l)+f(l+1)) + 9 (f(l-2)+...+f(l+2)), so any
+    sum of consecutive interior differences telescopes to (G(b) - G(a-1))/1920
+    for random half-node values.  (The one-sided closures at l = 1, 2, n-1, n,
+    which the reference applies at every block end, interfaces included, do
+    not telescope: a periodic box's summed residual is not zero.)"""
+    rng = np.random.default_rng(7)
+    ni = 24
+    f = np.ascontiguousarray(rng.standard_normal(ni + 1))
+    df = np.zeros(ni)
+    L.orc_flux_dxyz(1, ni, _p(f), _p(df))
+    G = lambda l: 2250 * f[l] - 125 * (f[l - 1] + f[l] + f[l + 1]) + 9 * (f[l - 2] + f[l - 1] + f[l] + f[l + 1] + f[l + 2])
+    for a, b in ((3, ni - 2), (5, 11), (4, 4)):
+        lhs = float(np.sum(df[a - 1:b]))
+        rhs = (G(b) - G(a - 1)) / 1920.0
+        assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(rhs)), (a, b, lhs, rhs)
