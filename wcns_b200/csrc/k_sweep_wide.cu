@@ -24,13 +24,16 @@
 // latency of the hop between SMs.
 //
 // Inputs are re-laid plane-major by k_wide_prep (once per step): for every
-// cell its prim, the nine metrics, the three inviscid and three viscous
-// spectral radii and coed (getcoed, 602-645), and rhs = dq
-// (store_rhs_nb, 1592-1613); the cells of one chunk and plane are contiguous
-// in every array, so a warp's loads are coalesced and one bulk prefetch per
-// array brings a chunk's next planes into L2.  The split-Jacobian
-// coefficients are evaluated from them before the plane barrier, off the
-// dependency chain.  lusgs_l stores its dq for lusgs_u; lusgs_u stores the
+// cell the dq-independent split-Jacobian coefficients of both signs (from
+// its prim, nine metrics and inviscid spectral radii), coed (getcoed,
+// 602-645), the viscous radii, and rhs = dq (store_rhs_nb, 1592-1613); the
+// cells of one chunk and plane are contiguous in every array, so a warp's
+// loads are coalesced.  A thread issues its cell's loads at the top of the
+// plane, before the plane barrier, off the dependency chain.  (Neither an L2
+// prefetch of the next planes by one thread, nor per-thread prefetches, nor
+// staging the words in shared memory with cp.async, one plane ahead or not,
+// made the sweeps faster on the SA channel: all of them were slower.)
+// lusgs_l stores its dq for lusgs_u; lusgs_u stores the
 // terms it received from its upper neighbours -- evaluated with their final
 // dq they are the old-side terms of gs_pr_l (der, dfr, dgr); gs_pr_l stores
 // the sum of the terms it received from its lower neighbours, the old side of
@@ -55,7 +58,8 @@ namespace {
 enum : int { WS_SH = 0, WS_D = 6, WS_P = 18, WS_MN = 27, WS_COED = 36, WS_SRV = 37, WS_N = 40 };
 static_assert(WS_N == WIDE_COEF_WORDS, "coefficient words per slot");
 constexpr int WIDE_RING = 8;
-constexpr int WIDE_PREFETCH = 3;  // planes prefetched into L2 ahead of the one being swept
+constexpr int WIDE_PREFETCH = 3;  // planes prefetched into L2 ahead of the one being swept (SA sweep)
+constexpr int PREP_DS = 4;        // planes per column that neighbouring lanes of a prep kernel take
 
 // The chunk's slots t = (k-1)*w + jj (j = j0+jj+1) that hold a cell of plane
 // p, i.e. 1 <= p-j-k <= ni: the first and last of them (the range between
@@ -128,9 +132,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed(unsigned *p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
+// publishes every write that the CTA made before its last __syncthreads():
+// the barrier orders the other threads' writes before this thread's fence,
+// and fence.acq_rel.gpu followed by a relaxed store is a release pattern at
+// GPU scope, cumulative over what the barrier ordered before it (a
+// fence.sc.gpu, __threadfence(), costs about a microsecond more per plane)
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;\n" ::: "memory"); }
 // waits until *p >= want; gives up after `limit` clock cycles.  `seen` is the
 // largest count this thread has acquired from *p so far: a count it has
 // already seen needs no new load (the acquire that saw it orders every
@@ -166,10 +176,16 @@ __global__ void __launch_bounds__(256) k_wide_prep(DevParams P, DevFields F, con
     const WideChunk C = chunks[blockIdx.y];
     const DevBlock B = blocks[C.blk];
     const int ncolc = C.w * B.nk, np = B.ni + B.nj + B.nk - 2;
-    const long long n = (long long)np * ncolc;
+    const long long n = (long long)((np + PREP_DS - 1) / PREP_DS * PREP_DS) * ncolc;
     const double gama = P.gama;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int s = (int)(e / ncolc), t = (int)(e - (long long)s * ncolc);
+        // PREP_DS consecutive planes of one column per group of lanes: their
+        // cells are consecutive in i, so a group's gathers from the field
+        // layout share sectors, while a plane's stores stay runs of columns
+        const long long sb = e / ((long long)PREP_DS * ncolc);
+        const int r = (int)(e - sb * PREP_DS * ncolc), t = r / PREP_DS;
+        const int s = (int)sb * PREP_DS + (r - t * PREP_DS);
+        if (s >= np) continue;
         const int p = s + 3, j = C.j0 + t % C.w + 1, k = t / C.w + 1, i = p - j - k;
         if (i < 1 || i > B.ni) continue;
         const long long id = gidx(B, i, j, k);
@@ -258,24 +274,6 @@ __global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F
     for (int m = 0; m < NC; m++) ibuf[m] = 0.0;
     const int pfirst = FWD ? 3 : B.ni + B.nj + B.nk;
     const int pstep = FWD ? 1 : -1;
-    // the words this sweep reads: [first word, count] runs of the coefficient
-    // array, then the start values and the stored Gauss-Seidel terms
-    const int sg = FWD ? WS_P : WS_MN;
-    const double *warr[6] = {A.stat + (size_t)WS_SH * A.n, A.stat + (size_t)sg * A.n,
-                             A.stat + (size_t)WS_COED * A.n, MODE == 1 ? A.dql : A.rhs,
-                             MODE == 2 ? A.gs1 : MODE == 3 ? A.gs2 : nullptr, nullptr};
-    const int wcnt[6] = {WS_D + 12 - WS_SH, 9, LU ? 4 : 1, 5, MODE == 2 ? 15 : MODE == 3 ? 5 : 0, 0};
-    auto prefetch_plane = [&](int s) {
-        if (s >= np) return;
-        const int p = pfirst + s * pstep;
-        int lo, hi;
-        if (!active_slots(p, C.j0, C.w, B.ni, B.nk, lo, hi)) return;
-        const long long pm0 = C.pmoff + (long long)(p - 3) * ncol + (long long)C.j0 * B.nk + lo;
-        for (int a = 0; a < 5; a++)
-            for (int w = 0; w < wcnt[a]; w++) prefetch_l2(warr[a] + (size_t)w * A.n + pm0, hi - lo + 1);
-    };
-    if (t == 0)
-        for (int a = 0; a < WIDE_PREFETCH; a++) prefetch_plane(a);
     unsigned seen_prod = 0, seen_cons = 0;
     for (int s = 0; s < np; s++) {
         const int p = pfirst + s * pstep;
@@ -317,16 +315,15 @@ __global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F
             for (int m = 0; m < 5; m++) base[m] = bsrc[(size_t)m * A.n + pm];
         }
         if (t == 0) {
-            prefetch_plane(s + WIDE_PREFETCH);
             if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit(), seen_prod)) timed_out = true;
             if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit(), seen_cons))
                 timed_out = true;
         }
         __syncthreads();  // the previous plane's inbox and ring entries are complete
         if (t == 0 && (ring_out || ring_in)) {
-            __threadfence();
-            if (ring_out && s > 0) st_release(prod_out, (unsigned)s);      // planes 0..s-1 published
-            if (ring_in && s > 1) st_release(cons_in, (unsigned)(s - 1));  // planes 0..s-2 read
+            fence_acq_rel_gpu();
+            if (ring_out && s > 0) st_relaxed(prod_out, (unsigned)s);      // planes 0..s-1 published
+            if (ring_in && s > 1) st_relaxed(cons_in, (unsigned)(s - 1));  // planes 0..s-2 read
         }
         if (!act) continue;
         const double *rd = smem + (size_t)((s + 1) & 1) * half;
@@ -432,9 +429,9 @@ __global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F
     }
     __syncthreads();
     if (t == 0) {
-        __threadfence();
-        if (ring_out) st_release(prod_out, (unsigned)np);
-        if (ring_in) st_release(cons_in, (unsigned)np);
+        fence_acq_rel_gpu();
+        if (ring_out) st_relaxed(prod_out, (unsigned)np);
+        if (ring_in) st_relaxed(cons_in, (unsigned)np);
         if (timed_out) atomicAdd(&err[ERR_TIMEOUT], 1);
     }
 }
@@ -586,9 +583,15 @@ __global__ void __launch_bounds__(256) k_sa_wide_prep(DevFields F, SaFields S, c
     const WideChunk C = chunks[blockIdx.y];
     const DevBlock B = blocks[C.blk];
     const int ncolc = C.w * B.nk, np = B.ni + B.nj + B.nk - 2;
-    const long long n = (long long)np * ncolc;
+    const long long n = (long long)((np + PREP_DS - 1) / PREP_DS * PREP_DS) * ncolc;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int s = (int)(e / ncolc), t = (int)(e - (long long)s * ncolc);
+        // PREP_DS consecutive planes of one column per group of lanes: their
+        // cells are consecutive in i, so a group's gathers from the field
+        // layout share sectors, while a plane's stores stay runs of columns
+        const long long sb = e / ((long long)PREP_DS * ncolc);
+        const int r = (int)(e - sb * PREP_DS * ncolc), t = r / PREP_DS;
+        const int s = (int)sb * PREP_DS + (r - t * PREP_DS);
+        if (s >= np) continue;
         const int p = s + 3, j = C.j0 + t % C.w + 1, k = t / C.w + 1, i = p - j - k;
         if (i < 2 || i > B.ni - 1 || j < 2 || j > B.nj - 1 || k < 2 || k > B.nk - 1) continue;
         const long long id = gidx(B, i, j, k);
@@ -612,6 +615,11 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields 
     const DevBlock B = blocks[C.blk];
     const int t = threadIdx.x, ncolc = C.w * B.nk, ncol = B.nj * B.nk;
     const bool own = t < ncolc;
+    // the thread that waits on and publishes the ring counters: an idle lane
+    // when the CTA has one, so that no column's cell waits behind it (this
+    // scalar sweep gains 11 % on the SA channel; the mean-flow sweeps, whose
+    // idle lanes share a warp with busy ones, do not, and keep thread 0)
+    const int tc = ncolc < (int)blockDim.x ? (int)blockDim.x - 1 : 0;
     const int jj = own ? t % C.w : 0;
     const int j = C.j0 + jj + 1, k = own ? t / C.w + 1 : 1;
     const bool colin = own && j >= 2 && j <= B.nj - 1 && k >= 2 && k <= B.nk - 1;
@@ -660,16 +668,16 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields 
             base = A.sa[(size_t)(FWD ? WSA_RHS : WSA_FWD) * A.n + pm];
         }
         prefetch_plane(s + WIDE_PREFETCH);
-        if (t == 0) {
+        if (t == tc) {
             if (ring_in && s > 0 && !wait_count(prod_in, (unsigned)s, limit(), seen_prod)) timed_out = true;
             if (ring_out && s >= WIDE_RING && !wait_count(cons_out, (unsigned)(s - WIDE_RING + 1), limit(), seen_cons))
                 timed_out = true;
         }
         __syncthreads();
-        if (t == 0 && (ring_out || ring_in)) {
-            __threadfence();
-            if (ring_out && s > 0) st_release(prod_out, (unsigned)s);
-            if (ring_in && s > 1) st_release(cons_in, (unsigned)(s - 1));
+        if (t == tc && (ring_out || ring_in)) {
+            fence_acq_rel_gpu();
+            if (ring_out && s > 0) st_relaxed(prod_out, (unsigned)s);
+            if (ring_in && s > 1) st_relaxed(cons_in, (unsigned)(s - 1));
         }
         if (!act) continue;
         const int rp = (s + 1) & 1, wp = s & 1;
@@ -690,10 +698,10 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields 
         if (jedge_out && ring_out) __stcg(ring_out + ((size_t)(s % WIDE_RING) * A.nkmax + (k - 1)) * 10, l[1] * nw);
     }
     __syncthreads();
-    if (t == 0) {
-        __threadfence();
-        if (ring_out) st_release(prod_out, (unsigned)np);
-        if (ring_in) st_release(cons_in, (unsigned)np);
+    if (t == tc) {
+        fence_acq_rel_gpu();
+        if (ring_out) st_relaxed(prod_out, (unsigned)np);
+        if (ring_in) st_relaxed(cons_in, (unsigned)np);
         if (timed_out) atomicAdd(&err[ERR_TIMEOUT], 1);
     }
 }

@@ -78,8 +78,10 @@ struct ProfMarks {
 
 // Wide sweeps (k_sweep_wide.cu): a chunk of whole j-rows of one block per
 // CTA, plane-major arrays, rings of planes between neighbouring chunks.
-constexpr int WIDE_MAX_THREADS = 576;
-constexpr int WIDE_MAX_REGS = 112;  // 18 warps x 32 x 112 registers fit one SM's register file
+constexpr int WIDE_MAX_THREADS = 512;
+// 16 warps x 32 x 128 registers fill one SM's register file, four warps of
+// 4,096 registers per sub-partition
+constexpr int WIDE_MAX_REGS = 128;
 constexpr int WIDE_COEF_WORDS = 40;  // coefficient words per slot (k_sweep_wide.cu)
 struct WideChunk {
     int blk, j0, w;         // block (0-based), first j-row (0-based) and width of the chunk
