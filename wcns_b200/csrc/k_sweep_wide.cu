@@ -320,7 +320,11 @@ __global__ void __maxnreg__(WIDE_MAX_REGS) k_sweep_wide(DevParams P, DevFields F
                 timed_out = true;
         }
         __syncthreads();  // the previous plane's inbox and ring entries are complete
-        if (t == 0 && (ring_out || ring_in)) {
+        // the counters move at every second plane: half the fences on thread
+        // 0's path, and a consumer that sees two planes per acquire, for one
+        // more plane of lag per chunk boundary (3.76 -> 3.56 ms for the four
+        // sweeps of the SA channel; every third plane is no better)
+        if (t == 0 && (ring_out || ring_in) && (s & 1) == 0) {
             fence_acq_rel_gpu();
             if (ring_out && s > 0) st_relaxed(prod_out, (unsigned)s);      // planes 0..s-1 published
             if (ring_in && s > 1) st_relaxed(cons_in, (unsigned)(s - 1));  // planes 0..s-2 read
@@ -674,7 +678,7 @@ __global__ void __launch_bounds__(WIDE_MAX_THREADS, 1) k_sa_sweep_wide(SaFields 
                 timed_out = true;
         }
         __syncthreads();
-        if (t == tc && (ring_out || ring_in)) {
+        if (t == tc && (ring_out || ring_in) && (s & 1) == 0) {  // every second plane, as in the mean-flow sweeps
             fence_acq_rel_gpu();
             if (ring_out && s > 0) st_relaxed(prod_out, (unsigned)s);
             if (ring_in && s > 1) st_relaxed(cons_in, (unsigned)(s - 1));
