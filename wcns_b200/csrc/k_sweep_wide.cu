@@ -79,41 +79,6 @@ struct Jsh {  // direction-independent part
     double um, vm, wm, hm, c2, af;
 };
 
-// the dq-independent part of mxdq_std (gettmhmgm_ns GasModel.f90:411-426,
-// nt = 0) from s = prim (5), the nine metrics, the three inviscid radii
-__device__ __forceinline__ void jac_coeffs(double gama, const double *s, int d, double npn, Jsh &H, Jsc &J) {
-    const double rm = s[0], um = s[1], vm = s[2], wm = s[3], pm = s[4];
-    const double nt = 0.0;
-    const double hint = gama / (gama - 1.0) * pm / rm;
-    const double c2 = gama * pm / rm;
-    const double cm = sqrt(c2);
-    const double v2 = um * um + vm * vm + wm * wm;
-    H.um = um;
-    H.vm = vm;
-    H.wm = wm;
-    H.hm = hint + 0.5 * v2;
-    H.c2 = c2;
-    const double ae = gama - 1.0;
-    H.af = 0.5 * ae * v2;
-    double nx = s[5 + 3 * d], ny = s[5 + 3 * d + 1], nz = s[5 + 3 * d + 2];
-    const double rad = s[14 + d];
-    double ct = nx * um + ny * vm + nz * wm + nt;
-    double cgm = sqrt(nx * nx + ny * ny + nz * nz);
-    if (!(cgm >= SML_SSS)) cgm = SML_SSS;
-    double l1 = ct, l4 = ct + cm * cgm, l5 = ct - cm * cgm;
-    l1 = 0.5 * (l1 + npn * rad);
-    l4 = 0.5 * (l4 + npn * rad);
-    l5 = 0.5 * (l5 + npn * rad);
-    J.x1 = (2.0 * l1 - l4 - l5) / (2.0 * c2);
-    J.x2 = (l4 - l5) / (2.0 * cm);
-    J.l1 = l1;
-    const double cgm1 = 1.0 / cgm;
-    J.nx = nx * cgm1;
-    J.ny = ny * cgm1;
-    J.nz = nz * cgm1;
-    J.ct = (ct - nt) * cgm1;
-}
-
 // the dq-dependent part of mxdq_std
 __device__ __forceinline__ void jac_apply_w(double gama, const Jsh &H, const Jsc &J, const double *dq, double *f) {
     const double ae = gama - 1.0;
@@ -170,8 +135,10 @@ __device__ __forceinline__ void prefetch_l2(const double *ptr, int n) {
 // neighbour (getrkec_mml and getrarbrc return the cell's own metrics and
 // spectral radius for interior cells) for both signs, coed (getcoed,
 // 602-645), the viscous radii, and rhs = dq (set_nonconnect_boundary_dq_0
-// has run, so rhs holds the zeros of the physical faces); one thread per slot
-__global__ void __launch_bounds__(256) k_wide_prep(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+// has run, so rhs holds the zeros of the physical faces); one thread per
+// slot, four CTAs of 256 threads per SM (64 registers: 0.95 ms per channel
+// step, against 1.02 at two CTAs per SM and 1.18 at 108 registers)
+__global__ void __launch_bounds__(256, 4) k_wide_prep(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                   const WideChunk *__restrict__ chunks, WideArrays A) {
     const WideChunk C = chunks[blockIdx.y];
     const DevBlock B = blocks[C.blk];
@@ -192,36 +159,46 @@ __global__ void __launch_bounds__(256) k_wide_prep(DevParams P, DevFields F, con
         const long long pm = C.pmoff + (long long)s * (B.nj * B.nk) + (long long)C.j0 * B.nk + t;
         double *o = A.stat + pm;
         const size_t N = (size_t)A.n;
-        double st[21];  // prim, metrics, inviscid radii
-#pragma unroll
-        for (int m = 0; m < 5; m++) st[m] = F.f[F_R + m][id];
-#pragma unroll
-        for (int m = 0; m < 9; m++) st[5 + m] = F.f[F_KCX + m][id];
-#pragma unroll
-        for (int m = 0; m < 3; m++) st[14 + m] = F.f[F_SRA + m][id];
-        Jsh H;
-#pragma unroll
+        // the dq-independent part of mxdq_std (gettmhmgm_ns GasModel.f90:411-426,
+        // nt = 0) from the prim, the nine metrics and the three inviscid
+        // radii, each value stored as soon as it is known so that few are
+        // live at a time
+        const double rm = F.f[F_R][id], um = F.f[F_U][id], vm = F.f[F_V][id], wm = F.f[F_W][id], pres = F.f[F_P][id];
+        const double nt = 0.0;
+        const double hint = gama / (gama - 1.0) * pres / rm;
+        const double c2 = gama * pres / rm;
+        const double cm = sqrt(c2);
+        const double v2 = um * um + vm * vm + wm * wm;
+        const double ae = gama - 1.0;
+        o[(WS_SH + 0) * N] = um;
+        o[(WS_SH + 1) * N] = vm;
+        o[(WS_SH + 2) * N] = wm;
+        o[(WS_SH + 3) * N] = hint + 0.5 * v2;
+        o[(WS_SH + 4) * N] = c2;
+        o[(WS_SH + 5) * N] = 0.5 * ae * v2;
+#pragma unroll 1
         for (int d = 0; d < 3; d++) {
-            Jsc Jp, Jm;
-            jac_coeffs(gama, st, d, 1.0, H, Jp);
-            jac_coeffs(gama, st, d, -1.0, H, Jm);
-            o[(WS_D + 4 * d + 0) * N] = Jp.nx;
-            o[(WS_D + 4 * d + 1) * N] = Jp.ny;
-            o[(WS_D + 4 * d + 2) * N] = Jp.nz;
-            o[(WS_D + 4 * d + 3) * N] = Jp.ct;
-            o[(WS_P + 3 * d + 0) * N] = Jp.l1;
-            o[(WS_P + 3 * d + 1) * N] = Jp.x1;
-            o[(WS_P + 3 * d + 2) * N] = Jp.x2;
-            o[(WS_MN + 3 * d + 0) * N] = Jm.l1;
-            o[(WS_MN + 3 * d + 1) * N] = Jm.x1;
-            o[(WS_MN + 3 * d + 2) * N] = Jm.x2;
+            const double nx = F.f[F_KCX + 3 * d][id], ny = F.f[F_KCX + 3 * d + 1][id], nz = F.f[F_KCX + 3 * d + 2][id];
+            const double rad = F.f[F_SRA + d][id];
+            const double ct = nx * um + ny * vm + nz * wm + nt;
+            double cgm = sqrt(nx * nx + ny * ny + nz * nz);
+            if (!(cgm >= SML_SSS)) cgm = SML_SSS;
+            const double l1 = ct, l4 = ct + cm * cgm, l5 = ct - cm * cgm;
+#pragma unroll
+            for (int sg = 0; sg < 2; sg++) {
+                const double npn = sg == 0 ? 1.0 : -1.0;
+                const double a1 = 0.5 * (l1 + npn * rad), a4 = 0.5 * (l4 + npn * rad), a5 = 0.5 * (l5 + npn * rad);
+                const int w0 = sg == 0 ? WS_P : WS_MN;
+                o[(w0 + 3 * d + 0) * N] = a1;
+                o[(w0 + 3 * d + 1) * N] = (2.0 * a1 - a4 - a5) / (2.0 * c2);
+                o[(w0 + 3 * d + 2) * N] = (a4 - a5) / (2.0 * cm);
+            }
+            const double cgm1 = 1.0 / cgm;
+            o[(WS_D + 4 * d + 0) * N] = nx * cgm1;
+            o[(WS_D + 4 * d + 1) * N] = ny * cgm1;
+            o[(WS_D + 4 * d + 2) * N] = nz * cgm1;
+            o[(WS_D + 4 * d + 3) * N] = (ct - nt) * cgm1;
         }
-        o[(WS_SH + 0) * N] = H.um;
-        o[(WS_SH + 1) * N] = H.vm;
-        o[(WS_SH + 2) * N] = H.wm;
-        o[(WS_SH + 3) * N] = H.hm;
-        o[(WS_SH + 4) * N] = H.c2;
-        o[(WS_SH + 5) * N] = H.af;
         // getcoed (LHS.f90:602-645), wmig = beta = 1, no dual time stepping
         double rad_ns = F.f[F_SRA][id] + F.f[F_SRB][id] + F.f[F_SRC][id];
         if (P.nvis >= 1) rad_ns = rad_ns + F.f[F_SRVA][id] + F.f[F_SRVB][id] + F.f[F_SRVC][id];
