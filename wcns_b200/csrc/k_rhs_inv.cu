@@ -153,9 +153,13 @@ __device__ __forceinline__ double qwl_preright(const InvLine &L, const double *s
 }
 
 // out == nullptr: dq += dF in place; otherwise dF is stored in
-// out[m*stride + point] for an ordered combine (k_combine_dq)
+// out[m*stride + point] for an ordered combine (k_combine_dq).  Four CTAs
+// per SM (64 registers, with some spill; at most 54 KB of staged lines):
+// 3.52 ms per channel step for the three directions against 3.62 at three
+// CTAs of 80 registers.  (The viscous kernel at four 256-thread CTAs of 64
+// registers spills 0.5 KB per thread and runs 4.1 ms against 3.4.)
 template <int dir>
-__global__ void __launch_bounds__(256, 3) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
+__global__ void __launch_bounds__(256, 4) k_rhs_invis(DevParams P, DevFields F, const DevBlock *__restrict__ blocks,
                                                    const LineGroup *__restrict__ groups, int *err, double *out,
                                                    long long stride) {
     extern __shared__ double smem[];
