@@ -324,8 +324,9 @@ static int build_line_tables(WcnsContext *c, int inv_cap, int vis_cap) {
                 size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : pass == 1 ? rhs_vis_line_bytes(n)
                                 : pass == 2 ? rhs_invis_mx_line_bytes(n) : rhs_vis_mx_line_bytes(n);
                 // staged lines per CTA: at most 54 KB for the FP64 inviscid kernel (four
-                // 256-thread CTAs of 64 registers per SM), 72 KB for the others (three
-                // 256-thread inviscid or two 384-thread viscous CTAs of 80 registers)
+                // 256-thread CTAs of 64 registers per SM), 72 KB for the others (two
+                // 320-thread FP64 viscous CTAs of 96 registers; the mixed-precision
+                // kernels' own shapes)
                 int NL = pass == 0 ? std::max(1, std::min({std::min(inv_cap, rhs_invis_max_lines()), 3072 / (5 * (n + 2)),
                                                            (int)((54 * 1024) / per_line)}))
                        : pass == 1 ? std::max(1, std::min({std::min(vis_cap, rhs_vis_max_lines()), 512 / (n + 1), (int)((72 * 1024) / per_line)}))
