@@ -1374,7 +1374,7 @@ static int enqueue_step(WcnsContext *c, double *rms_slot) {
     }
     launch_rhs_dirs(L, false);
     for (int d = 0; d < 3; d++) n += L.inv[d].ngroups ? 1 : 0;
-    n += (L.inv[1].ngroups || L.inv[2].ngroups) ? 1 : 0;
+    n += (L.mixed && (L.inv[1].ngroups || L.inv[2].ngroups)) ? 1 : 0;  // k_combine_dq (the FP64 directions add in place)
     prof_mark(L, "rhs_invis");
     launch_communicate(L, 0); n += L.nsnap ? 2 : 0;
     prof_mark(L, "communicate_dq");
