@@ -428,15 +428,3 @@ def test_adjoint_solve_by_gmres_converges_where_the_fixed_point_grows():
     hist, rel, fixed = _gmres_and_fixed_point("box_roe", restart=40, maxiter=1500, tol=1e-9)
     assert hist[-1] <= 1e-9 and rel <= 1e-8
     assert fixed > 1.0
-
-
-def test_adjoint_solve_by_gmres_outpaces_the_fixed_point_on_the_plate():
-    """The eight-block Euler plate: the fixed point creeps (3e-2 of its start
-    after 2,000 steps); GMRES(250) is far ahead after the same number of
-    operator applications (1e-4 to 5e-5 on the B200).  The system is badly
-    conditioned (the solution for a random g grows to 1e7 while r_Q^T psi
-    stays O(1)), so two applications of the operator to psi, whose sums run
-    in different orders through atomics, differ by up to a few tenths of a
-    per cent of the small residual: the fresh check is bounded, not matched."""
-    hist, rel, fixed = _gmres_and_fixed_point("plate_euler", restart=250, maxiter=2000, tol=1e-9)
-    assert hist[-1] < 0.1 * fixed and rel < 0.1 * fixed
