@@ -324,15 +324,34 @@ static int build_line_tables(WcnsContext *c, int inv_cap, int vis_cap) {
                 size_t per_line = pass == 0 ? rhs_invis_line_bytes(n) : pass == 1 ? rhs_vis_line_bytes(n)
                                 : pass == 2 ? rhs_invis_mx_line_bytes(n) : rhs_vis_mx_line_bytes(n);
                 // staged lines per CTA: at most 54 KB for the FP64 inviscid kernel (four
-                // 256-thread CTAs of 64 registers per SM), 72 KB for the others (two
-                // 320-thread FP64 viscous CTAs of 96 registers; the mixed-precision
-                // kernels' own shapes)
+                // 256-thread CTAs of 64 registers per SM), 108 KB for the FP64 viscous
+                // kernel (two 320-thread CTAs of 96 registers), 72 KB for the
+                // mixed-precision kernels
                 int NL = pass == 0 ? std::max(1, std::min({std::min(inv_cap, rhs_invis_max_lines()), 3072 / (5 * (n + 2)),
                                                            (int)((54 * 1024) / per_line)}))
-                       : pass == 1 ? std::max(1, std::min({std::min(vis_cap, rhs_vis_max_lines()), 512 / (n + 1), (int)((72 * 1024) / per_line)}))
+                       : pass == 1 ? std::max(1, std::min({std::min(vis_cap, rhs_vis_max_lines()), 512 / (n + 1), (int)((108 * 1024) / per_line)}))
                        : pass == 2 ? std::max(1, std::min({std::min(inv_cap, rhs_invis_mx_max_lines()), 3072 / (5 * (n + 2)),
                                                            (int)((72 * 1024) / per_line)}))
                                    : std::max(1, std::min({std::min(vis_cap, rhs_vis_mx_max_lines()), 512 / (n + 1), (int)((72 * 1024) / per_line)}));
+                if (pass == 1) {
+                    // the FP64 viscous kernel's heavy phase has one item per (line, half
+                    // node): of NL/2..NL lines take the count whose items fill the last
+                    // pass of the CTA's threads best, so that few threads idle at the
+                    // barrier after it (3.29 -> 3.11 ms per channel step with the larger
+                    // staging limit)
+                    const int thr = rhs_vis_threads();
+                    int best = NL;
+                    double best_fill = 0.0;
+                    for (int q = NL; q >= std::max(1, (NL + 1) / 2); q--) {
+                        const int items = q * (n + 1), rounds = (items + thr - 1) / thr;
+                        const double fill = (double)items / ((double)rounds * thr);
+                        if (fill > best_fill + 1e-9) {
+                            best_fill = fill;
+                            best = q;
+                        }
+                    }
+                    NL = best;
+                }
                 for (int bb = 1; bb <= nb2; bb++)
                     for (int a = 1; a <= na; a += NL) {
                         LineGroup lg{b, a, bb, std::min(NL, na - a + 1)};

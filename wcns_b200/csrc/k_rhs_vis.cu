@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(VIS_THREADS, 2) k_rhs_vis(DevParams P, DevFiel
 
 size_t rhs_vis_line_bytes(int n) { return (size_t)vis_line_stride(n) * 8; }
 int rhs_vis_max_lines() { return VIS_MAX_LINES; }
+int rhs_vis_threads() { return VIS_THREADS; }
 
 void launch_rhs_vis(const LaunchCtx &c, int dir, cudaStream_t st, double *out) {
     if (c.mixed) return launch_rhs_vis_mx(c, dir, st, out);

@@ -228,6 +228,7 @@ void launch_rhs_dirs(const LaunchCtx &c, bool vis);
 void setup_rhs_vis_attrs(size_t max_smem);
 size_t rhs_vis_line_bytes(int n);  // shared memory of one line in k_rhs_vis
 int rhs_vis_max_lines();           // lines per CTA in k_rhs_vis
+int rhs_vis_threads();            // threads per CTA in k_rhs_vis
 // mixed-precision residual (k_rhs_mixed.cu)
 void launch_rhs_invis_mx(const LaunchCtx &c, int dir, cudaStream_t st, double *out);
 void launch_rhs_vis_mx(const LaunchCtx &c, int dir, cudaStream_t st, double *out);
